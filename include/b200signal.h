@@ -1,0 +1,129 @@
+/*
+ * b200signal: C-ABI of the B200 (sm_100a) framed-FFT spectral kernels.
+ *
+ * Every entry point takes raw device pointers, plain sizes and a CUDA stream (cudaStream_t
+ * passed as void*), launches asynchronously on that stream and returns an int status
+ * (SP_OK = 0, negative on error; sp_last_error() gives the text of the calling thread's last
+ * error). Nothing here synchronises the device, allocates device memory or falls back to a
+ * CPU path: shapes the kernels do not cover return SP_ERR_UNSUPPORTED.
+ *
+ * The functions replace the kernel-module boundary of the reference library
+ * (src/mlx_signal_processing/_stft_metal.py and _fourstep_metal.py): Python functions that
+ * take MLX arrays plus integers and launch JIT-compiled Metal kernels. Citations below are to
+ * those files. Windows arrive with the scipy scale factor already folded in (sqrt(scale) for
+ * PSD/CSD, as at src/mlx_signal_processing/spectral.py:312-316).
+ *
+ * Layout conventions: a signal is `rows` rows of `n` float32 samples with row stride `ld`
+ * (elements); complex outputs are interleaved (re, im) float32 pairs (complex64).
+ */
+#ifndef B200SIGNAL_H
+#define B200SIGNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SP_API __attribute__((visibility("default")))
+#else
+#define SP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SP_VERSION 100
+
+enum {
+  SP_OK = 0,
+  SP_ERR_ARG = -1,          /* invalid argument (null pointer, bad size) */
+  SP_ERR_UNSUPPORTED = -2,  /* shape outside the fused kernels (e.g. non power-of-two nfft) */
+  SP_ERR_WORKSPACE = -3,    /* workspace smaller than the size query returned */
+  SP_ERR_CUDA = -4,         /* CUDA runtime error (text in sp_last_error) */
+  SP_ERR_TIMEOUT = -5       /* a bounded device-side wait gave up */
+};
+
+enum { SP_DETREND_NONE = 0, SP_DETREND_CONSTANT = 1, SP_DETREND_LINEAR = 2 };
+
+/* Library version (SP_VERSION). */
+SP_API int sp_version(void);
+
+/* Text of the calling thread's last error ("" if none). */
+SP_API const char* sp_last_error(void);
+
+/*
+ * Workspace bytes for sp_welch_f32 (kind 0) or sp_csd_c64 / sp_coherence_f32 (kind 1) on the
+ * current device. Negative return = error status.
+ * Replaces the implicit group-partial buffers of _stft_metal.rfft_power_mean
+ * (_stft_metal.py:530-557) and _pair_sum_launch (_stft_metal.py:703-736).
+ */
+SP_API int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
+                               int detrend);
+
+/*
+ * Welch PSD: out[r][k] = (onesided ? f_k : 1) / nseg * sum_s |FFT_nfft(win * detrend(x_rs))_k|^2
+ * for k < (onesided ? nfft/2+1 : nfft), segments x_rs = x[r, s*hop : s*hop+nperseg].
+ * nfft must be a power of two in [1, 4096] with nperseg <= nfft; win holds nperseg values.
+ * Replaces _stft_metal.rfft_power_mean (_stft_metal.py:530-557) together with the deferred
+ * one-sided factor of spectral.csd (spectral.py:468-488).
+ */
+SP_API int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
+                 int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
+                 void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Cross spectral density mean conj(X_s) Y_s over segments (complex64 out, same bin count and
+ * one-sided doubling as sp_welch_f32). Replaces _stft_metal.csd_mean (_stft_metal.py:739-741).
+ */
+SP_API int sp_csd_c64(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+               int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
+               int onesided, float* out, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Magnitude-squared coherence |Pxy|^2 / (Pxx Pyy) from one sweep (float32 out, nfft/2+1 bins),
+ * guarded (0 where Pxx Pyy == 0) and clamped to [0, 1]. Replaces _stft_metal.coherence_mean
+ * (_stft_metal.py:744-746) plus the unguarded ratio of spectral.coherence (spectral.py:609-613).
+ */
+SP_API int sp_coherence_f32(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+                     int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
+                     float* out, void* workspace, size_t workspace_bytes, void* stream);
+
+
+/* Boundary extension modes of the per-frame entry points (scipy stft `boundary`). */
+enum { SP_EXT_NONE = 0, SP_EXT_ZEROS = 1, SP_EXT_EVEN = 2, SP_EXT_ODD = 3, SP_EXT_CONSTANT = 4 };
+
+/*
+ * Per-frame windowed FFT (stft). The signal is virtually extended by `ext` samples per side
+ * with `ext_mode` and zero-padded to `n_total` (>= n + 2*ext); frame s covers extended samples
+ * [s*hop, s*hop + nperseg). Output: (rows, nseg, nbins) complex64, nseg = (n_total-nperseg)/hop+1,
+ * nbins = onesided ? nfft/2+1 : nfft. Replaces _stft_metal.rfft_frames(power=False)
+ * (_stft_metal.py:192-220) and the materialised boundary/pad concatenates of
+ * spectral._spectral_helper (spectral.py:275-288).
+ */
+SP_API int sp_stft_c64(const float* x, int64_t rows, int64_t n, int64_t ld, int ext, int ext_mode,
+                       int64_t n_total, const float* win, int nperseg, int nfft, int hop,
+                       int detrend, int onesided, float* out, void* stream);
+
+/*
+ * Per-frame power |X|^2 with the one-sided doubling applied (spectrogram mode 'psd'), same
+ * framing and layout as sp_stft_c64 (float32 out). Replaces _stft_metal.rfft_frames(power=True)
+ * (_stft_metal.py:192-220) plus the one-sided factor of spectral.py:348-353.
+ */
+SP_API int sp_spectrogram_f32(const float* x, int64_t rows, int64_t n, int64_t ld, int ext,
+                              int ext_mode, int64_t n_total, const float* win, int nperseg,
+                              int nfft, int hop, int detrend, int onesided, float* out,
+                              void* stream);
+
+/*
+ * Per-frame cross spectra conj(X_s) Y_s, (rows, nseg, nbins) complex64, no one-sided factor.
+ * Replaces _stft_metal.csd_frames (_stft_metal.py:412-414), used for average='median'.
+ */
+SP_API int sp_csd_frames_c64(const float* x, const float* y, int64_t rows, int64_t n,
+                             int64_t ldx, int64_t ldy, const float* win, int nperseg, int nfft,
+                             int hop, int detrend, int onesided, float* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200SIGNAL_H */

@@ -1,0 +1,139 @@
+"""Typed launchers over the C-ABI: torch CUDA tensors in, torch CUDA tensors out.
+
+Each launcher validates layout, allocates the output and the workspace through torch's caching
+allocator, and launches on torch's current stream. This is the counterpart of the reference's
+kernel-module functions (src/mlx_signal_processing/_stft_metal.py: rfft_power_mean :530,
+csd_mean :739, coherence_mean :744).
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+from ._array import stream_handle
+
+#: largest nfft served by the fused segment kernels
+MAX_FUSED_NFFT = 4096
+
+DETREND_CODES = {False: 0, None: 0, "constant": 1, "c": 1, "linear": 2, "l": 2}
+
+
+def is_pow2(v: int) -> bool:
+    return v >= 1 and (v & (v - 1)) == 0
+
+
+def fused_mean_ok(nfft: int) -> bool:
+    return is_pow2(nfft) and nfft <= MAX_FUSED_NFFT
+
+
+def _rows(x: torch.Tensor) -> tuple[torch.Tensor, int]:
+    """2-D float32 CUDA view with unit inner stride; returns (tensor, row stride)."""
+    assert x.dim() == 2 and x.is_cuda and x.dtype == torch.float32
+    if x.stride(1) != 1 or (x.shape[0] > 1 and x.stride(0) < x.shape[1]):
+        x = x.contiguous()
+    ld = x.stride(0) if x.shape[0] > 1 else x.shape[1]
+    return x, max(int(ld), x.shape[1])
+
+
+def _workspace(nbytes: int, dev: torch.device) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=dev)
+
+
+def welch_mean(x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop: int,
+               detrend: int, onesided: bool) -> torch.Tensor:
+    """Mean |FFT(win * detrend(segment))|^2 over segments of each row of x -> (rows, nout)."""
+    x, ld = _rows(x)
+    rows, n = x.shape
+    lib = _lib.load()
+    ws_bytes = lib.sp_mean_workspace_size(0, rows, n, nperseg, nfft, hop, detrend)
+    if ws_bytes < 0:
+        _lib.check(int(ws_bytes), "sp_mean_workspace_size")
+    nout = nfft // 2 + 1 if onesided else nfft
+    out = torch.empty((rows, nout), dtype=torch.float32, device=x.device)
+    ws = _workspace(ws_bytes, x.device)
+    _lib.check(
+        lib.sp_welch_f32(x.data_ptr(), rows, n, ld, win.data_ptr(), nperseg, nfft, hop, detrend,
+                         int(onesided), out.data_ptr(), ws.data_ptr(), ws.numel(),
+                         stream_handle()),
+        "sp_welch_f32",
+    )
+    return out
+
+
+def cross_mean(mode: str, x: torch.Tensor, y: torch.Tensor, win: torch.Tensor, nperseg: int,
+               nfft: int, hop: int, detrend: int, onesided: bool = True) -> torch.Tensor:
+    """mode 'csd': mean conj(X)Y (complex64, one-sided doubling if requested);
+    mode 'coherence': |Pxy|^2/(Pxx Pyy) (float32)."""
+    x, ldx = _rows(x)
+    y, ldy = _rows(y)
+    assert x.shape == y.shape
+    rows, n = x.shape
+    lib = _lib.load()
+    ws_bytes = lib.sp_mean_workspace_size(1, rows, n, nperseg, nfft, hop, detrend)
+    if ws_bytes < 0:
+        _lib.check(int(ws_bytes), "sp_mean_workspace_size")
+    ws = _workspace(ws_bytes, x.device)
+    if mode == "csd":
+        nout = nfft // 2 + 1 if onesided else nfft
+        out = torch.empty((rows, nout), dtype=torch.complex64, device=x.device)
+        _lib.check(
+            lib.sp_csd_c64(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy, win.data_ptr(),
+                           nperseg, nfft, hop, detrend, int(onesided), out.data_ptr(),
+                           ws.data_ptr(), ws.numel(), stream_handle()),
+            "sp_csd_c64",
+        )
+        return out
+    if mode == "coherence":
+        out = torch.empty((rows, nfft // 2 + 1), dtype=torch.float32, device=x.device)
+        _lib.check(
+            lib.sp_coherence_f32(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy, win.data_ptr(),
+                                 nperseg, nfft, hop, detrend, out.data_ptr(), ws.data_ptr(),
+                                 ws.numel(), stream_handle()),
+            "sp_coherence_f32",
+        )
+        return out
+    raise ValueError(mode)
+
+
+EXT_CODES = {None: 0, "zeros": 1, "even": 2, "odd": 3, "constant": 4}
+
+
+def frames(kind: str, x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop: int,
+           detrend: int, onesided: bool, ext: int = 0, ext_mode=None, n_total: int | None = None,
+           y: torch.Tensor | None = None) -> torch.Tensor:
+    """Per-frame spectra of each row: (rows, nseg, nbins).
+
+    kind 'stft' -> complex64 X_s; 'power' -> float32 |X_s|^2 with one-sided doubling;
+    'cross' -> complex64 conj(X_s) Y_s (no doubling). Boundary extension (`ext` samples per
+    side, scipy `boundary` mode `ext_mode`) and zero padding up to `n_total` are virtual.
+    """
+    x, ldx = _rows(x)
+    rows, n = x.shape
+    n_total = n + 2 * ext if n_total is None else int(n_total)
+    nseg = (n_total - nperseg) // hop + 1
+    nbins = nfft // 2 + 1 if onesided else nfft
+    lib = _lib.load()
+    if kind == "power":
+        out = torch.empty((rows, nseg, nbins), dtype=torch.float32, device=x.device)
+        _lib.check(lib.sp_spectrogram_f32(x.data_ptr(), rows, n, ldx, ext, EXT_CODES[ext_mode],
+                                          n_total, win.data_ptr(), nperseg, nfft, hop, detrend,
+                                          int(onesided), out.data_ptr(), stream_handle()),
+                   "sp_spectrogram_f32")
+        return out
+    out = torch.empty((rows, nseg, nbins), dtype=torch.complex64, device=x.device)
+    if kind == "stft":
+        _lib.check(lib.sp_stft_c64(x.data_ptr(), rows, n, ldx, ext, EXT_CODES[ext_mode], n_total,
+                                   win.data_ptr(), nperseg, nfft, hop, detrend, int(onesided),
+                                   out.data_ptr(), stream_handle()),
+                   "sp_stft_c64")
+        return out
+    if kind == "cross":
+        assert y is not None and ext == 0 and n_total == n
+        y, ldy = _rows(y)
+        _lib.check(lib.sp_csd_frames_c64(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy,
+                                         win.data_ptr(), nperseg, nfft, hop, detrend,
+                                         int(onesided), out.data_ptr(), stream_handle()),
+                   "sp_csd_frames_c64")
+        return out
+    raise ValueError(kind)

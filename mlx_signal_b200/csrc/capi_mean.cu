@@ -1,0 +1,202 @@
+// C-ABI: segment-mean spectral estimates (welch / csd / coherence).
+#include <utility>
+
+#include "capi_common.h"
+#include "dispatch.cuh"
+
+namespace b2s {
+namespace {
+
+constexpr int kMaxLog = kMaxLogL;
+
+}  // namespace
+
+__global__ void k_reduce_mean(ReduceParams p) {
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= p.rows * p.nout) return;
+  const int64_t r = idx / p.nout;
+  const int k = int(idx - r * p.nout);
+  const int L = p.L;
+  const int kk = (L - k) & (L - 1);
+  const int kc = k <= kk ? k : kk;
+  const int64_t t0 = first_team(r, p.nseg, p.G);
+  int64_t t1 = last_team(r, p.nseg, p.G);
+  if (t1 > p.nteams - 1) t1 = p.nteams - 1;
+  const int nsl = int(t1 - t0 + 1);
+  double fac = 1.0 / double(p.nseg);
+  if (p.onesided && k != 0 && 2 * k != L) fac *= 2.0;
+  if (p.mode == 0) {
+    const float* base = p.partial + r * p.cmax * int64_t(L);
+    double s = 0.0;
+    for (int c = 0; c < nsl; ++c) {
+      const float* q = base + int64_t(c) * L;
+      s += double(q[k]) + double(q[kk]);
+    }
+    p.out[idx] = float(0.5 * s * fac);
+    return;
+  }
+  const int stride = cross_slot_floats(L);
+  const int cq = cross_q_floats(L);
+  const float* base = p.partial + r * p.cmax * int64_t(stride);
+  double qk = 0.0, qm = 0.0, cr = 0.0, ci = 0.0;
+  for (int c = 0; c < nsl; ++c) {
+    const float* q = base + int64_t(c) * stride;
+    qk += double(q[k]);
+    qm += double(q[kk]);
+    cr += double(q[cq + 2 * kc]);
+    ci += double(q[cq + 2 * kc + 1]);
+  }
+  const double pxy_re = 0.5 * ci, pxy_im = 0.25 * (qm - qk);
+  if (p.mode == 1) {
+    p.out[2 * idx] = float(pxy_re * fac);
+    p.out[2 * idx + 1] = float(pxy_im * fac);
+    return;
+  }
+  const double sxx = 0.25 * (qk + qm + 2.0 * cr);
+  const double syy = 0.25 * (qk + qm - 2.0 * cr);
+  const double num = pxy_re * pxy_re + pxy_im * pxy_im;
+  const double den = sxx * syy;
+  double coh = den > 0.0 ? num / den : 0.0;
+  if (!(coh >= 0.0)) coh = 0.0;
+  if (coh > 1.0) coh = 1.0;
+  p.out[idx] = float(coh);
+}
+
+
+namespace {
+
+struct MeanPlanInfo {
+  MeanInfo k;
+  int log_l = 0;
+  int nseg = 0;
+  int64_t total = 0, G = 0, nteams = 0, blocks = 0;
+  int cmax = 0;
+  int64_t slot_floats = 0;
+  int64_t ws_bytes = 0;
+};
+
+int make_plan(bool cross, int64_t rows, int64_t n, int nperseg, int nfft, int hop, int detrend,
+              MeanPlanInfo* pl) {
+  if (rows < 0 || n < 1 || nperseg < 1 || nperseg > n || hop < 1 || hop > nperseg ||
+      nfft < nperseg || detrend < 0 || detrend > 2 || n >= (int64_t(1) << 31)) {
+    set_error("invalid spectral-mean arguments (rows=%lld n=%lld nperseg=%d nfft=%d hop=%d)",
+              (long long)rows, (long long)n, nperseg, nfft, hop);
+    return SP_ERR_ARG;
+  }
+  const int log_l = ilog2_exact(nfft);
+  if (log_l < 0 || log_l > kMaxLog) {
+    set_error("nfft=%d: fused kernels need a power of two <= %d", nfft, 1 << kMaxLog);
+    return SP_ERR_UNSUPPORTED;
+  }
+  pl->k = cross ? mean_lookup_cross(log_l, detrend) : mean_lookup_welch(log_l, detrend);
+  pl->log_l = log_l;
+  pl->nseg = int((n - nperseg) / hop + 1);
+  pl->total = rows * pl->nseg;
+  int sms = 0;
+  const int nb = resident_ctas(pl->k.fn, pl->k.threads, pl->k.smem, &sms);
+  if (nb <= 0) {
+    set_error("no resident CTA for spectral-mean kernel (nfft=%d, smem=%zu)", nfft, pl->k.smem);
+    return SP_ERR_UNSUPPORTED;
+  }
+  const int64_t cap = int64_t(nb) * sms * pl->k.teams;
+  const int64_t total = pl->total > 0 ? pl->total : 1;
+  pl->G = cross ? cdiv(total, cap) : 2 * cdiv(total, 2 * cap);
+  if (pl->G < 1) pl->G = 1;
+  pl->nteams = cdiv(total, pl->G);
+  pl->blocks = cdiv(pl->nteams, pl->k.teams);
+  int64_t cm = cdiv(pl->nseg, pl->G) + 1;
+  if (cm > pl->nteams) cm = pl->nteams;
+  pl->cmax = int(cm);
+  const int64_t L = int64_t(1) << log_l;
+  pl->slot_floats = cross ? cross_slot_floats(int(L)) : L;
+  pl->ws_bytes = rows * pl->cmax * pl->slot_floats * int64_t(sizeof(float));
+  return SP_OK;
+}
+
+int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+             int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
+             int onesided, float* out, void* ws, size_t ws_bytes, void* stream) {
+  const bool cross = mode != 0;
+  if (!x || !win || !out || (cross && !y) || ldx < n || (cross && ldy < n)) {
+    set_error("null pointer or row stride smaller than n");
+    return SP_ERR_ARG;
+  }
+  MeanPlanInfo pl;
+  int st = make_plan(cross, rows, n, nperseg, nfft, hop, detrend, &pl);
+  if (st != SP_OK) return st;
+  if (rows == 0) return SP_OK;
+  if (ws_bytes < size_t(pl.ws_bytes) || (pl.ws_bytes > 0 && !ws)) {
+    set_error("workspace too small: need %lld bytes, got %zu", (long long)pl.ws_bytes, ws_bytes);
+    return SP_ERR_WORKSPACE;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  MeanParams p;
+  p.x = x;
+  p.y = y;
+  p.ld_x = ldx;
+  p.ld_y = cross ? ldy : 0;
+  p.rows = rows;
+  p.nperseg = nperseg;
+  p.hop = hop;
+  p.nseg = pl.nseg;
+  p.detrend = detrend;
+  p.win = win;
+  p.G = pl.G;
+  p.cmax = pl.cmax;
+  p.total = pl.total;
+  p.partial = static_cast<float*>(ws);
+  pl.k.launch(dim3(unsigned(pl.blocks)), pl.k.threads, pl.k.smem, s, p);
+  B2S_CHECK_CUDA(cudaGetLastError(), "spectral-mean kernel launch");
+  ReduceParams rp;
+  rp.partial = p.partial;
+  rp.rows = rows;
+  rp.L = nfft;
+  rp.nout = (mode == 2 || onesided) ? nfft / 2 + 1 : nfft;
+  rp.onesided = (mode != 2 && onesided) ? 1 : 0;
+  rp.nseg = pl.nseg;
+  rp.G = pl.G;
+  rp.cmax = pl.cmax;
+  rp.nteams = pl.nteams;
+  rp.mode = mode;
+  rp.out = out;
+  const int64_t nthr = rows * rp.nout;
+  const int tb = 256;
+  k_reduce_mean<<<unsigned(cdiv(nthr, tb)), tb, 0, s>>>(rp);
+  B2S_CHECK_CUDA(cudaGetLastError(), "spectral-mean reduce launch");
+  return SP_OK;
+}
+
+}  // namespace
+}  // namespace b2s
+
+extern "C" {
+
+int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
+                               int detrend) {
+  b2s::MeanPlanInfo pl;
+  const int st = b2s::make_plan(kind != 0, rows, n, nperseg, nfft, hop, detrend, &pl);
+  return st == SP_OK ? pl.ws_bytes : int64_t(st);
+}
+
+int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
+                 int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
+                 void* workspace, size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(0, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, onesided,
+                       out, workspace, workspace_bytes, stream);
+}
+
+int sp_csd_c64(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+               int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
+               int onesided, float* out, void* workspace, size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(1, x, y, rows, n, ldx, ldy, win, nperseg, nfft, hop, detrend, onesided,
+                       out, workspace, workspace_bytes, stream);
+}
+
+int sp_coherence_f32(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+                     int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
+                     float* out, void* workspace, size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(2, x, y, rows, n, ldx, ldy, win, nperseg, nfft, hop, detrend, 1, out,
+                       workspace, workspace_bytes, stream);
+}
+
+}

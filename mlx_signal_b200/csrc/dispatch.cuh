@@ -1,0 +1,62 @@
+// Kernel dispatch tables shared by the split translation units (one TU per kernel family so
+// the template instantiations compile in parallel).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <utility>
+
+#include "frame_kernels.cuh"
+#include "mean_kernels.cuh"
+
+namespace b2s {
+
+// Points per thread for a team FFT of length 2^LOG_L: single-thread FFTs up to 32 points, then
+// teams of 8-128 threads with one register exchange for L = 256 and 1024.
+template <int LOG_L>
+constexpr int team_log_e() {
+  return LOG_L <= 5 ? LOG_L : (LOG_L == 6 ? 3 : (LOG_L <= 8 ? 4 : 5));
+}
+
+constexpr int kMaxLogL = 12;
+
+template <class P>
+using LaunchFnT = void (*)(dim3, int, size_t, cudaStream_t, const P&);
+
+template <class P>
+struct KernelInfo {
+  const void* fn = nullptr;
+  int threads = 0;
+  size_t smem = 0;
+  int teams = 0;
+  LaunchFnT<P> launch = nullptr;
+};
+
+using MeanInfo = KernelInfo<MeanParams>;
+using FrameInfo = KernelInfo<FrameParams>;
+
+// family: 0 welch mean, 1 cross mean
+MeanInfo mean_lookup_welch(int log_l, int det);
+MeanInfo mean_lookup_cross(int log_l, int det);
+FrameInfo frame_lookup_stft(int log_l, int det);
+FrameInfo frame_lookup_power(int log_l, int det);
+FrameInfo frame_lookup_cross(int log_l, int det);
+
+// Fold-expression lookup over LOG_L = 0..kMaxLogL and detrend 0..2 of an info factory.
+template <class INFO, template <int, int> class F, int... LS>
+INFO lookup_seq(int log_l, int det, std::integer_sequence<int, LS...>) {
+  INFO out;
+  (void)((log_l == LS ? (out = det == 0 ? F<LS, 0>::get()
+                                        : (det == 1 ? F<LS, 1>::get() : F<LS, 2>::get()),
+                         true)
+                      : false) ||
+         ...);
+  return out;
+}
+
+template <class INFO, template <int, int> class F>
+INFO lookup_all(int log_l, int det) {
+  return lookup_seq<INFO, F>(log_l, det, std::make_integer_sequence<int, kMaxLogL + 1>{});
+}
+
+}  // namespace b2s

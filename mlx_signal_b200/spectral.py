@@ -1,0 +1,654 @@
+"""Spectral estimation on B200: welch, csd, coherence, periodogram, spectrogram, stft, istft.
+
+scipy.signal-compatible signatures and semantics (same defaults, shapes, scaling and edge
+handling), following the reference's src/mlx_signal_processing/spectral.py. Inputs may be
+NumPy arrays, lists or torch tensors (CPU or CUDA); results are torch CUDA tensors (float32 or
+complex64). Computation is float32/complex64.
+
+Routing (the reference's `_stft_metal.eligible` rule, spectral.py:319-347, widened): real
+float32 input with a power-of-two nfft <= 4096 and detrend in {False, 'constant', 'linear'}
+runs the fused CUDA kernels (segment gather + detrend + window + FFT + |X|^2 or X conj(Y) +
+segment mean in one sweep). Other shapes (non-power-of-two nfft, complex input, median
+averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
+counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing runs on the CPU.
+"""
+
+from __future__ import annotations
+
+import functools
+import math
+import warnings
+
+import numpy as np
+import torch
+
+from . import _kernels
+from ._array import device, input_shape, input_size, to_device, to_numpy
+from ._config import composed_path_notice
+from .windows import _window_np, device_vector
+
+__all__ = ["coherence", "csd", "istft", "periodogram", "spectrogram", "stft", "welch"]
+
+_BOUNDARY_MODES = ("even", "odd", "constant", "zeros", None)
+
+
+# ---------------------------------------------------------------------------------------------
+# building blocks
+# ---------------------------------------------------------------------------------------------
+
+
+def _triage_segments(window, nperseg, input_length):
+    """Resolve (window values float64, nperseg) like scipy's _triage_segments
+    (reference spectral.py:45-69)."""
+    if isinstance(window, str | tuple):
+        nperseg = 256 if nperseg is None else int(nperseg)
+        if nperseg > input_length:
+            warnings.warn(
+                f"nperseg = {nperseg:d} is greater than input length "
+                f" = {input_length:d}, using nperseg = {input_length:d}",
+                stacklevel=4,
+            )
+            nperseg = input_length
+        key = tuple(window) if isinstance(window, tuple) else window
+        win_np = _window_np(key, nperseg)
+    else:
+        win_np = np.asarray(to_numpy(window), dtype=np.float64)
+        if win_np.ndim != 1:
+            raise ValueError("window must be 1-D")
+        if input_length < win_np.shape[0]:
+            raise ValueError("window is longer than input signal")
+        if nperseg is None:
+            nperseg = win_np.shape[0]
+        elif int(nperseg) != win_np.shape[0]:
+            raise ValueError("value specified for nperseg is different from length of window")
+        nperseg = int(nperseg)
+    return win_np, nperseg
+
+
+def _detrend_code(detrend) -> int:
+    if detrend is False or detrend is None:
+        return 0
+    if callable(detrend):
+        raise NotImplementedError(
+            "callable detrend has no GPU path in mlx_signal_b200 (pass False, 'constant' or "
+            "'linear')"
+        )
+    if not isinstance(detrend, str) or detrend not in ("constant", "c", "linear", "l"):
+        raise ValueError("Trend type must be 'linear' or 'constant'.")
+    return _kernels.DETREND_CODES[detrend]
+
+
+def _detrend_frames(d: torch.Tensor, code: int) -> torch.Tensor:
+    """Per-frame detrend on the last axis (composed path; reference spectral.py:89-104)."""
+    if code == 0:
+        return d
+    m = d.mean(dim=-1, keepdim=True)
+    if code == 1:
+        return d - m
+    n = d.shape[-1]
+    denom = n * (n * n - 1) / 12.0
+    if denom == 0.0:
+        return d - m
+    t = torch.arange(n, device=d.device, dtype=torch.float32) - (n - 1) / 2.0
+    slope = (d * t).sum(dim=-1, keepdim=True) / denom
+    return d - m - slope * t
+
+
+@functools.lru_cache(maxsize=64)
+def _onesided_factor_np(nfft: int) -> np.ndarray:
+    """[1, 2, ..., 2, (1 if nfft even else 2)]: one-sided PSD doubling (spectral.py:150-157)."""
+    f = np.full(nfft // 2 + 1, 2.0, dtype=np.float32)
+    f[0] = 1.0
+    if nfft % 2 == 0:
+        f[-1] = 1.0
+    return f
+
+
+def _median_bias(n: int) -> float:
+    ii_2 = 2 * np.arange(1.0, (n - 1) // 2 + 1)
+    return float(1 + np.sum(1.0 / (ii_2 + 1) - 1.0 / ii_2))
+
+
+def _median_last(a: torch.Tensor) -> torch.Tensor:
+    """numpy-style median over the last axis (mean of the two middle values if even)."""
+    n = a.shape[-1]
+    s, _ = torch.sort(a, dim=-1)
+    if n % 2:
+        return s[..., n // 2]
+    return 0.5 * (s[..., n // 2 - 1] + s[..., n // 2])
+
+
+def _unwrap(p: torch.Tensor, axis: int = -1) -> torch.Tensor:
+    """np.unwrap (period 2*pi) in torch ops (reference spectral.py:165-174)."""
+    p = p.movedim(axis, -1)
+    d = p[..., 1:] - p[..., :-1]
+    two_pi = 2.0 * math.pi
+    ddmod = torch.remainder(d + math.pi, two_pi) - math.pi
+    ddmod = torch.where((ddmod == -math.pi) & (d > 0), torch.full_like(ddmod, math.pi), ddmod)
+    ph_correct = torch.where(d.abs() < math.pi, torch.zeros_like(d), ddmod - d)
+    out = torch.cat([p[..., :1], p[..., 1:] + torch.cumsum(ph_correct, dim=-1)], dim=-1)
+    return out.movedim(-1, axis)
+
+
+def _empty(shape) -> torch.Tensor:
+    return torch.zeros(tuple(shape), dtype=torch.float32, device=device())
+
+
+def _freqs(nfft: int, fs: float, onesided: bool) -> torch.Tensor:
+    f = np.fft.rfftfreq(nfft, 1 / fs) if onesided else np.fft.fftfreq(nfft, 1 / fs)
+    return torch.from_numpy(f.astype(np.float32)).to(device())
+
+
+def _pad_last(t: torch.Tensor, n: int) -> torch.Tensor:
+    cur = t.shape[-1]
+    if cur == n:
+        return t
+    return torch.nn.functional.pad(t, (0, n - cur)) if not t.is_complex() else torch.cat(
+        [t, torch.zeros(t.shape[:-1] + (n - cur,), dtype=t.dtype, device=t.device)], dim=-1
+    )
+
+
+def _extend(t: torch.Tensor, mode: str, n: int) -> torch.Tensor:
+    """Edge extension by n samples on the last axis (reference _arraytools.py:16-52)."""
+    if n < 1 or mode is None:
+        return t
+    if mode != "constant" and mode != "zeros" and n > t.shape[-1] - 1:
+        raise ValueError(
+            f"The extension length n ({n}) is too big. It must not exceed "
+            f"x.shape[-1]-1, which is {t.shape[-1] - 1}."
+        )
+    if mode == "zeros":
+        z = torch.zeros(t.shape[:-1] + (n,), dtype=t.dtype, device=t.device)
+        return torch.cat([z, t, z], dim=-1)
+    if mode == "constant":
+        left = t[..., :1].expand(t.shape[:-1] + (n,))
+        right = t[..., -1:].expand(t.shape[:-1] + (n,))
+        return torch.cat([left, t, right], dim=-1)
+    left = t[..., 1 : n + 1].flip(-1)
+    right = t[..., -(n + 1) : -1].flip(-1)
+    if mode == "even":
+        return torch.cat([left, t, right], dim=-1)
+    return torch.cat([2 * t[..., :1] - left, t, 2 * t[..., -1:] - right], dim=-1)
+
+
+def _composed_spectra(X: torch.Tensor, win: torch.Tensor, code: int, nperseg: int, nstep: int,
+                      nfft: int, onesided: bool) -> torch.Tensor:
+    """Frames -> detrend -> window -> FFT on the GPU (cuFFT): (..., nseg, nfreq)."""
+    frames = X.unfold(-1, nperseg, nstep)
+    frames = _detrend_frames(frames, code) * win
+    if onesided:
+        return torch.fft.rfft(frames, n=nfft, dim=-1)
+    if not frames.is_complex():
+        frames = frames.to(torch.complex64)
+    return torch.fft.fft(frames, n=nfft, dim=-1)
+
+
+# ---------------------------------------------------------------------------------------------
+# shared argument handling (scipy _spectral_helper semantics, reference spectral.py:186-368)
+# ---------------------------------------------------------------------------------------------
+
+
+class _Setup:
+    pass
+
+
+def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling, axis,
+           mode, boundary, padded, same):
+    if mode not in ("psd", "stft"):
+        raise ValueError(f"Unknown value for mode {mode}, must be one of: ('psd', 'stft')")
+    if boundary not in _BOUNDARY_MODES:
+        raise ValueError(
+            f"Unknown boundary option '{boundary}', must be one of: "
+            f"{['even', 'odd', 'constant', 'zeros', None]}"
+        )
+    if not same and mode != "psd":
+        raise ValueError("x and y must be equal if mode is 'stft'")
+    axis = int(axis)
+    X = to_device(x)
+    Y = X if same else to_device(y)
+    s = _Setup()
+    s.empty = None
+    if not same:
+        xouter, youter = list(X.shape), list(Y.shape)
+        xouter.pop(axis)
+        youter.pop(axis)
+        try:
+            s.outershape = tuple(np.broadcast_shapes(tuple(xouter), tuple(youter)))
+        except ValueError as e:
+            raise ValueError("x and y cannot be broadcast together.") from e
+    if same:
+        if X.numel() == 0:
+            e = _empty(X.shape)
+            s.empty = (e, e, e)
+            return s
+    elif X.numel() == 0 or Y.numel() == 0:
+        outshape = s.outershape + (min(X.shape[axis], Y.shape[axis]),)
+        e = _empty(outshape).movedim(-1, axis)
+        s.empty = (e, e, e)
+        return s
+    if X.dim() > 1 and axis != -1:
+        X = X.movedim(axis, -1)
+        if not same and Y.dim() > 1:
+            Y = Y.movedim(axis, -1)
+    if not same and X.shape[-1] != Y.shape[-1]:
+        if X.shape[-1] < Y.shape[-1]:
+            X = _pad_last(X, Y.shape[-1])
+        else:
+            Y = _pad_last(Y, X.shape[-1])
+    if nperseg is not None:
+        nperseg = int(nperseg)
+        if nperseg < 1:
+            raise ValueError("nperseg must be a positive integer")
+    win_np, nperseg = _triage_segments(window, nperseg, input_length=X.shape[-1])
+    nfft = nperseg if nfft is None else int(nfft)
+    if nfft < nperseg:
+        raise ValueError("nfft must be greater than or equal to nperseg.")
+    noverlap = nperseg // 2 if noverlap is None else int(noverlap)
+    if noverlap >= nperseg:
+        raise ValueError("noverlap must be less than nperseg.")
+    nstep = nperseg - noverlap
+    code = _detrend_code(detrend)
+    n_orig = X.shape[-1]
+    ext = nperseg // 2 if boundary is not None else 0
+    if boundary is not None and boundary in ("even", "odd") and ext > n_orig - 1:
+        raise ValueError(
+            f"The extension length n ({ext}) is too big. It must not exceed "
+            f"x.shape[-1]-1, which is {n_orig - 1}."
+        )
+    n_ext = n_orig + 2 * ext
+    nadd = (-(n_ext - nperseg) % nstep) % nperseg if padded else 0
+    x_complex = X.is_complex()
+    y_complex = (not same) and Y.is_complex()
+    onesided = bool(return_onesided) and not (x_complex or y_complex)
+    if scaling == "density":
+        scale = 1.0 / (fs * float((win_np * win_np).sum()))
+    elif scaling == "spectrum":
+        scale = 1.0 / float(win_np.sum()) ** 2
+    else:
+        raise ValueError(f"Unknown scaling: {scaling!r}")
+    s.X, s.Y, s.same, s.axis = X, Y, same, axis
+    s.win_np, s.nperseg, s.nfft, s.noverlap, s.nstep = win_np, nperseg, nfft, noverlap, nstep
+    s.code, s.onesided, s.scale, s.fs = code, onesided, scale, fs
+    s.boundary, s.ext, s.n_orig, s.n_total = boundary, ext, n_orig, n_ext + nadd
+    s.win = device_vector((win_np * np.sqrt(scale)).astype(np.float32))
+    s.freqs = _freqs(nfft, fs, onesided)
+    t_np = np.arange(nperseg / 2, s.n_total - nperseg / 2 + 1, nstep) / float(fs)
+    if boundary is not None:
+        t_np = t_np - (nperseg / 2) / fs
+    s.t = torch.from_numpy(t_np.astype(np.float32)).to(device())
+    s.fused = (not x_complex) and (not y_complex) and _kernels.fused_mean_ok(nfft)
+    return s
+
+
+def _materialize_frames_input(s) -> tuple[torch.Tensor, torch.Tensor | None]:
+    """Boundary extension and padding applied explicitly (composed path only)."""
+    X, Y = s.X, s.Y
+    if s.boundary is not None:
+        X = _extend(X, s.boundary, s.ext)
+        if not s.same:
+            Y = _extend(Y, s.boundary, s.ext)
+    if s.n_total != X.shape[-1]:
+        X = _pad_last(X, s.n_total)
+        if not s.same:
+            Y = _pad_last(Y, s.n_total)
+    return X, (None if s.same else Y)
+
+
+def _freq_axis_out(result: torch.Tensor, axis: int) -> torch.Tensor:
+    """(..., nseg, nfreq) -> frequency axis at `axis`, time last (spectral.py:359-361)."""
+    ax = axis - 1 if axis < 0 else axis
+    return result.movedim(-1, ax)
+
+
+# ---------------------------------------------------------------------------------------------
+# public functions
+# ---------------------------------------------------------------------------------------------
+
+
+def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
+        detrend="constant", return_onesided=True, scaling="density", axis=-1, average="mean"):
+    """Cross power spectral density Pxy by Welch's method (scipy.signal.csd semantics).
+
+    Deviation from scipy: float32/complex64 compute; complex input switches to a two-sided
+    spectrum silently (as the reference does, spectral.py:290-298).
+    """
+    if average not in ("mean", "median"):
+        raise ValueError(f"average must be 'mean' or 'median', got {average!r}")
+    same = y is x
+    if input_size(x) == 0 or (not same and input_size(y) == 0):
+        xs = input_shape(x)
+        if same:
+            e = _empty(xs)
+            return e, e
+        ys = input_shape(y)
+        xo, yo = list(xs), list(ys)
+        xo.pop(axis)
+        yo.pop(axis)
+        outshape = tuple(np.broadcast_shapes(tuple(xo), tuple(yo))) + (min(xs[axis], ys[axis]),)
+        e = _empty(outshape).movedim(-1, axis)
+        return e, e
+    s = _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
+               axis, "psd", None, False, same)
+    if s.empty is not None:
+        return s.empty[0], s.empty[1]
+    X, Y = s.X, s.Y
+    outer = tuple(X.shape[:-1]) if same else s.outershape
+    n = X.shape[-1]
+    nseg = (n - s.nperseg) // s.nstep + 1
+    if s.fused and average == "mean":
+        rows = int(np.prod(outer)) if outer else 1
+        if same:
+            res = _kernels.welch_mean(X.reshape(rows, n), s.win, s.nperseg, s.nfft, s.nstep,
+                                      s.code, s.onesided)
+        else:
+            Xb = X.expand(outer + (n,)).reshape(rows, n)
+            Yb = Y.expand(outer + (n,)).reshape(rows, n)
+            res = _kernels.cross_mean("csd", Xb, Yb, s.win, s.nperseg, s.nfft, s.nstep, s.code,
+                                      s.onesided)
+        pxy = res.reshape(outer + (res.shape[-1],))
+    else:
+        rows = int(np.prod(outer)) if outer else 1
+        if s.fused:
+            # median averaging: per-frame fused kernels, then the order statistic
+            if same:
+                per = _kernels.frames("power", X.reshape(rows, n), s.win, s.nperseg, s.nfft,
+                                      s.nstep, s.code, False)
+                if s.onesided:
+                    per = per[..., : s.nfft // 2 + 1]
+            else:
+                Xb = X.expand(outer + (n,)).reshape(rows, n)
+                Yb = Y.expand(outer + (n,)).reshape(rows, n)
+                per = _kernels.frames("cross", Xb, s.win, s.nperseg, s.nfft, s.nstep, s.code,
+                                      s.onesided, y=Yb)
+            per = per.reshape(outer + per.shape[-2:])
+        else:
+            composed_path_notice("csd", "shape outside the fused kernels")
+            fx = _composed_spectra(X, s.win, s.code, s.nperseg, s.nstep, s.nfft, s.onesided)
+            if same:
+                per = fx.real.square() + fx.imag.square()
+            else:
+                fy = _composed_spectra(Y, s.win, s.code, s.nperseg, s.nstep, s.nfft, s.onesided)
+                per = torch.conj(fx) * fy
+        per = per.movedim(-2, -1)  # (..., nfreq, nseg)
+        if nseg > 1:
+            if average == "median":
+                bias = _median_bias(nseg)
+                if per.is_complex():
+                    pxy = torch.complex(_median_last(per.real), _median_last(per.imag))
+                else:
+                    pxy = _median_last(per)
+                pxy = pxy / bias
+            else:
+                pxy = per.mean(dim=-1)
+        else:
+            pxy = per[..., 0]
+        if s.onesided:
+            pxy = pxy * device_vector(_onesided_factor_np(s.nfft))
+    if pxy.dim() > 1 and s.axis != -1:
+        pxy = pxy.movedim(-1, s.axis if s.axis >= 0 else pxy.dim() + s.axis)
+    return s.freqs, pxy
+
+
+def welch(x, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
+          detrend="constant", return_onesided=True, scaling="density", axis=-1, average="mean"):
+    """Welch power spectral density (scipy.signal.welch semantics); the fused kernel computes
+    every segment's windowed FFT power and the segment mean of all channels in one sweep."""
+    freqs, pxx = csd(x, x, fs=fs, window=window, nperseg=nperseg, noverlap=noverlap, nfft=nfft,
+                     detrend=detrend, return_onesided=return_onesided, scaling=scaling,
+                     axis=axis, average=average)
+    if pxx.is_complex():
+        pxx = pxx.real
+    return freqs, pxx
+
+
+def periodogram(x, fs=1.0, window="boxcar", nfft=None, detrend="constant",
+                return_onesided=True, scaling="density", axis=-1):
+    """Power spectral density using a periodogram (scipy.signal.periodogram semantics,
+    reference spectral.py:529-578)."""
+    X = to_device(x)
+    if X.numel() == 0:
+        return _empty(X.shape), _empty(X.shape)
+    if window is None:
+        window = "boxcar"
+    n_ax = X.shape[axis]
+    if nfft is None:
+        nperseg = n_ax
+    elif nfft == n_ax:
+        nperseg = nfft
+    elif nfft > n_ax:
+        nperseg = n_ax
+    else:
+        X = X.narrow(axis, 0, nfft)
+        nperseg = nfft
+        nfft = None
+    if not isinstance(window, str | tuple) and window is not None:
+        if input_size(window) != nperseg:
+            raise ValueError(
+                "the size of the window must be the same size of the input on the specified axis"
+            )
+    return welch(X, fs=fs, window=window, nperseg=nperseg, noverlap=0, nfft=nfft,
+                 detrend=detrend, return_onesided=return_onesided, scaling=scaling, axis=axis)
+
+
+def coherence(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
+              detrend="constant", axis=-1):
+    """Magnitude-squared coherence |Pxy|^2/(Pxx Pyy) (scipy.signal.coherence semantics).
+
+    Fast path (equal-shape real inputs, power-of-two nfft): one fused sweep computes Pxx, Pyy
+    and Pxy together; scale factors cancel so the raw window is used (reference
+    spectral.py:591-617). The ratio is guarded (0 where Pxx*Pyy == 0) and clamped to [0, 1].
+    """
+    X, Y = to_device(x), to_device(y)
+    if (X.shape == Y.shape and not X.is_complex() and not Y.is_complex()
+            and X.dim() > 0 and X.shape[axis] > 0 and not callable(detrend)):
+        win_np, nps = _triage_segments(window, nperseg, input_length=X.shape[axis])
+        nov = nps // 2 if noverlap is None else int(noverlap)
+        nft = nps if nfft is None else int(nfft)
+        if nov < nps and nft >= nps and _kernels.fused_mean_ok(nft):
+            code = _detrend_code(detrend)
+            ax = axis % X.dim()
+            if X.dim() > 1 and ax != X.dim() - 1:
+                X = X.movedim(ax, -1)
+                Y = Y.movedim(ax, -1)
+            outer = tuple(X.shape[:-1])
+            rows = int(np.prod(outer)) if outer else 1
+            n = X.shape[-1]
+            win = device_vector(win_np.astype(np.float32))
+            cxy = _kernels.cross_mean("coherence", X.reshape(rows, n), Y.reshape(rows, n), win,
+                                      nps, nft, nps - nov, code)
+            cxy = cxy.reshape(outer + (cxy.shape[-1],))
+            if cxy.dim() > 1 and ax != cxy.dim() - 1:
+                cxy = cxy.movedim(-1, ax)
+            return _freqs(nft, fs, True), cxy
+    freqs, pxx = welch(X, fs=fs, window=window, nperseg=nperseg, noverlap=noverlap, nfft=nfft,
+                       detrend=detrend, axis=axis)
+    _, pyy = welch(Y, fs=fs, window=window, nperseg=nperseg, noverlap=noverlap, nfft=nfft,
+                   detrend=detrend, axis=axis)
+    _, pxy = csd(X, Y, fs=fs, window=window, nperseg=nperseg, noverlap=noverlap, nfft=nfft,
+                 detrend=detrend, axis=axis)
+    a = pxy.abs()
+    den = pxx * pyy
+    return freqs, torch.where(den > 0, a * a / torch.where(den > 0, den, 1.0), 0.0)
+
+
+def _frames_result(s, mode: str) -> torch.Tensor:
+    """Per-frame spectra (..., nseg, nfreq): complex (stft) or power (psd)."""
+    X = s.X
+    if s.fused:
+        outer = tuple(X.shape[:-1])
+        rows = int(np.prod(outer)) if outer else 1
+        n = X.shape[-1]
+        res = _kernels.frames("power" if mode == "psd" else "stft", X.reshape(rows, n), s.win,
+                              s.nperseg, s.nfft, s.nstep, s.code, s.onesided, ext=s.ext,
+                              ext_mode=s.boundary, n_total=s.n_total)
+        return res.reshape(outer + res.shape[-2:])
+    composed_path_notice("stft", "shape outside the fused kernels")
+    X, _ = _materialize_frames_input(s)
+    fx = _composed_spectra(X, s.win, s.code, s.nperseg, s.nstep, s.nfft, s.onesided)
+    if mode == "psd":
+        res = fx.real.square() + fx.imag.square()
+        if s.onesided:
+            res = res * device_vector(_onesided_factor_np(s.nfft))
+        return res
+    return fx
+
+
+def spectrogram(x, fs=1.0, window=("tukey", 0.25), nperseg=None, noverlap=None, nfft=None,
+                detrend="constant", return_onesided=True, scaling="density", axis=-1,
+                mode="psd"):
+    """Spectrogram (scipy.signal.spectrogram semantics: tukey window, nperseg//8 overlap)."""
+    modelist = ["psd", "complex", "magnitude", "angle", "phase"]
+    if mode not in modelist:
+        raise ValueError(f"unknown value for mode {mode}, must be one of {modelist}")
+    X = to_device(x)
+    window, nperseg = _triage_segments(window, nperseg, input_length=X.shape[axis])
+    if noverlap is None:
+        noverlap = nperseg // 8
+    helper_mode = "psd" if mode == "psd" else "stft"
+    s = _setup(X, X, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
+               axis, helper_mode, None, False, True)
+    if s.empty is not None:
+        return s.empty
+    sxx = _freq_axis_out(_frames_result(s, helper_mode), s.axis)
+    if mode == "magnitude":
+        sxx = sxx.abs()
+    elif mode in ("angle", "phase"):
+        sxx = torch.atan2(sxx.imag, sxx.real)
+        if mode == "phase":
+            ax = s.axis - 1 if s.axis < 0 else s.axis
+            sxx = _unwrap(sxx, axis=ax)
+    return s.freqs, s.t, sxx
+
+
+def stft(x, fs=1.0, window="hann", nperseg=256, noverlap=None, nfft=None, detrend=False,
+         return_onesided=True, boundary="zeros", padded=True, axis=-1, scaling="spectrum"):
+    """Short-time Fourier transform (legacy scipy.signal.stft semantics)."""
+    if scaling == "psd":
+        scaling = "density"
+    elif scaling != "spectrum":
+        raise ValueError(f"Parameter {scaling=} not in ['spectrum', 'psd']!")
+    s = _setup(x, x, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
+               axis, "stft", boundary, padded, True)
+    if s.empty is not None:
+        return s.empty
+    return s.freqs, s.t, _freq_axis_out(_frames_result(s, "stft"), s.axis)
+
+
+def _istft_axes(shape, freq_axis: int, time_axis: int):
+    """Validate and normalise istft axes -> (freq_ax, time_ax, perm) (spectral.py:766-785)."""
+    ndim = len(shape)
+    if ndim < 2:
+        raise ValueError("Input stft must be at least 2d!")
+    if freq_axis == time_axis:
+        raise ValueError("Must specify differing time and frequency axes!")
+    _ = shape[time_axis]
+    _ = shape[freq_axis]
+    freq_ax = freq_axis + ndim if freq_axis < 0 else freq_axis
+    time_ax = time_axis + ndim if time_axis < 0 else time_axis
+    if freq_ax == time_ax:
+        raise ValueError("Must specify differing time and frequency axes!")
+    zouter = [i for i in range(ndim) if i != freq_ax and i != time_ax]
+    return freq_ax, time_ax, zouter + [time_ax, freq_ax]
+
+
+_NOLA_CACHE: dict = {}
+
+
+def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
+          input_onesided=True, boundary=True, time_axis=-1, freq_axis=-2, scaling="spectrum"):
+    """Inverse short-time Fourier transform (scipy.signal.istft semantics).
+
+    Deviation (as in the reference, spectral.py:837-841): for N-d input the returned time
+    vector has the length of the output time axis.
+    """
+    freq_axis = int(freq_axis)
+    time_axis = int(time_axis)
+    shape = input_shape(Zxx)
+    freq_ax, time_ax, perm = _istft_axes(shape, freq_axis, time_axis)
+    Z = to_device(Zxx)
+    if perm != list(range(Z.dim())):
+        Z = Z.permute(perm)
+    if not Z.is_complex():
+        Z = Z.to(torch.complex64)
+    nseg = Z.shape[-2]
+    nf = Z.shape[-1]
+    n_default = 2 * (nf - 1) if input_onesided else nf
+    if nperseg is None:
+        nperseg = n_default
+    else:
+        nperseg = int(nperseg)
+        if nperseg < 1:
+            raise ValueError("nperseg must be a positive integer")
+    if nfft is None:
+        if input_onesided and (nperseg == n_default + 1):
+            nfft = nperseg
+        else:
+            nfft = n_default
+    elif nfft < nperseg:
+        raise ValueError("nfft must be greater than or equal to nperseg.")
+    else:
+        nfft = int(nfft)
+    noverlap = nperseg // 2 if noverlap is None else int(noverlap)
+    if noverlap >= nperseg:
+        raise ValueError("noverlap must be less than nperseg.")
+    nstep = nperseg - noverlap
+    if isinstance(window, str | tuple):
+        key = tuple(window) if isinstance(window, tuple) else window
+        win_np = _window_np(key, nperseg)
+    else:
+        win_np = np.asarray(to_numpy(window), dtype=np.float64)
+        if win_np.ndim != 1:
+            raise ValueError("window must be 1-D")
+        if win_np.shape[0] != nperseg:
+            raise ValueError(f"window must have length of {nperseg}")
+    if scaling == "spectrum":
+        scale = float(win_np.sum())
+    elif scaling == "psd":
+        scale = float(np.sqrt(fs * (win_np**2).sum()))
+    else:
+        raise ValueError(f"Parameter {scaling=} not in ['spectrum', 'psd']!")
+    outputlength = nperseg + (nseg - 1) * nstep
+    composed_path_notice("istft", "composed inverse path")
+    if input_onesided:
+        xsubs = torch.fft.irfft(Z, n=nfft, dim=-1)[..., :nperseg]
+    else:
+        xsubs = torch.fft.ifft(Z, n=nfft, dim=-1)[..., :nperseg]
+    win = device_vector(win_np.astype(np.float32))
+    xsubs = xsubs * (win * np.float32(scale))
+    batch = xsubs.shape[:-2]
+    v = xsubs.reshape((-1, nseg, nperseg)).transpose(1, 2)  # (B, nperseg, nseg)
+    fold = torch.nn.functional.fold
+    if v.is_complex():
+        xr = fold(v.real.contiguous(), (1, outputlength), (1, nperseg), stride=(1, nstep))
+        xi = fold(v.imag.contiguous(), (1, outputlength), (1, nperseg), stride=(1, nstep))
+        x = torch.complex(xr, xi)
+    else:
+        x = fold(v.contiguous(), (1, outputlength), (1, nperseg), stride=(1, nstep))
+    x = x.reshape(batch + (outputlength,))
+    w2 = (win * win).reshape(1, nperseg, 1).expand(1, nperseg, nseg).contiguous()
+    norm = fold(w2, (1, outputlength), (1, nperseg), stride=(1, nstep)).reshape(outputlength)
+    if boundary:
+        x = x[..., nperseg // 2 : -(nperseg // 2)]
+        norm = norm[nperseg // 2 : -(nperseg // 2)]
+    nola_key = (win_np.tobytes(), nperseg, nstep, nseg, outputlength, bool(boundary))
+    nola_ok = _NOLA_CACHE.get(nola_key)
+    if nola_ok is None:
+        nola_ok = bool((norm > 1e-10).all().item())
+        if len(_NOLA_CACHE) >= 256:
+            _NOLA_CACHE.clear()
+        _NOLA_CACHE[nola_key] = nola_ok
+    if not nola_ok:
+        warnings.warn(
+            "NOLA condition failed, STFT may not be invertible."
+            + (" Possibly due to missing boundary" if not boundary else ""),
+            stacklevel=2,
+        )
+    x = x / torch.where(norm > 1e-10, norm, torch.ones_like(norm))
+    if input_onesided and x.is_complex():
+        x = x.real
+    n_out = x.shape[-1]
+    out_time_axis = time_ax - (1 if freq_ax < time_ax else 0)
+    if x.dim() > 1 and out_time_axis != x.dim() - 1:
+        x = x.movedim(-1, out_time_axis)
+    time = torch.arange(n_out, dtype=torch.float32, device=x.device) / float(fs)
+    return time, x

@@ -1,0 +1,212 @@
+"""GPU parity: spectrogram / stft / istft against float64 scipy.signal.
+
+Cases follow the reference's tests/test_spectral.py (spectrogram modes, STFT_CASES boundary /
+padded / scaling, ISTFT_CASES, batched, layouts, arbitrary axes, validation, round trip) and
+test_metal_fft_workaround.py:97-131 (fused frames kernel vs a frame-by-frame oracle for odd hops).
+"""
+
+import numpy as np
+import pytest
+import scipy.signal as sps
+import torch
+
+import mlx_signal_b200 as msig
+from _utils import assert_close, make_sig
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mode", ["psd", "complex", "magnitude", "angle", "phase"])
+def test_spectrogram_matches_scipy(rng, mode):
+    x = make_sig(rng, (4096,))
+    f_ref, t_ref, s_ref = sps.spectrogram(x.astype(np.float64), fs=100.0, mode=mode)
+    f, t, s = msig.spectrogram(x, fs=100.0, mode=mode)
+    assert s_ref.shape == tuple(s.shape)
+    assert_close(f, f_ref)
+    assert_close(t, t_ref)
+    if mode in ("angle", "phase"):
+        mag = np.abs(sps.spectrogram(x.astype(np.float64), fs=100.0, mode="complex")[2])
+        keep = mag > 1e-4 * mag.max()
+        a = s.cpu().numpy()[keep]
+        d = s_ref[keep]
+        diff = np.angle(np.exp(1j * (a - d)))
+        np.testing.assert_allclose(diff, np.zeros_like(diff), atol=2e-3)
+    else:
+        assert_close(s, s_ref, rtol=2e-4)
+
+
+def test_spectrogram_custom_params(rng):
+    x = make_sig(rng, (4096,))
+    kw = dict(nperseg=200, noverlap=50, nfft=256, scaling="spectrum", detrend="linear")
+    f_ref, t_ref, s_ref = sps.spectrogram(x.astype(np.float64), **kw)
+    f, t, s = msig.spectrogram(x, **kw)
+    assert_close(s, s_ref)
+
+
+STFT_CASES = [
+    {},
+    {"nperseg": 128},
+    {"nperseg": 128, "noverlap": 100},
+    {"nperseg": 128, "nfft": 256},
+    {"boundary": "even"},
+    {"boundary": "odd"},
+    {"boundary": "constant"},
+    {"boundary": None},
+    {"padded": False},
+    {"scaling": "psd"},
+    {"detrend": "constant"},
+    {"return_onesided": False},
+]
+
+
+@pytest.mark.parametrize("case", STFT_CASES)
+def test_stft_matches_scipy(rng, case):
+    x = make_sig(rng, (4000,))
+    f_ref, t_ref, z_ref = sps.stft(x.astype(np.float64), fs=8000.0, **case)
+    f, t, z = msig.stft(x, fs=8000.0, **case)
+    assert z_ref.shape == tuple(z.shape)
+    assert_close(f, f_ref)
+    assert_close(t, t_ref)
+    assert_close(z, z_ref)
+
+
+def test_stft_multidim_axis0(rng):
+    x = make_sig(rng, (3000, 4))
+    f_ref, t_ref, z_ref = sps.stft(x.astype(np.float64), axis=0)
+    f, t, z = msig.stft(x, axis=0)
+    assert z_ref.shape == tuple(z.shape)
+    assert_close(z, z_ref)
+
+
+def test_stft_complex_input(rng):
+    x = make_sig(rng, (2048,), complex_=True)
+    with pytest.warns(UserWarning):
+        f_ref, t_ref, z_ref = sps.stft(x.astype(np.complex128))
+    f, t, z = msig.stft(x)
+    assert_close(z, z_ref)
+
+
+@pytest.mark.parametrize(
+    "n,N,hop,detrend",
+    [(5000, 256, 100, False), (5000, 256, 100, "constant"), (40000, 1024, 512, "constant"),
+     (40000, 2048, 320, False), (3000, 64, 7, "constant"), (9000, 4096, 1000, "linear")],
+)
+def test_fused_frames_match_frame_oracle(rng, n, N, hop, detrend):
+    """Fused per-frame kernel vs float64 frame-by-frame FFT with a random window (the
+    reference's fused-vs-composed check, test_metal_fft_workaround.py:97-131)."""
+    x = rng.standard_normal((3, n)).astype(np.float32)
+    win = rng.standard_normal(N).astype(np.float32)
+    nseg = (n - N) // hop + 1
+    idx = np.arange(N)[None, :] + hop * np.arange(nseg)[:, None]
+    fr = x.astype(np.float64)[:, idx]
+    if detrend:
+        fr = sps.detrend(fr, type=detrend, axis=-1)
+    ref = np.fft.rfft(fr * win.astype(np.float64), axis=-1)
+    from mlx_signal_b200 import _kernels
+    code = _kernels.DETREND_CODES[detrend]
+    xt = torch.from_numpy(x).cuda()
+    wt = torch.from_numpy(win).cuda()
+    got = _kernels.frames("stft", xt, wt, N, N, hop, code, True).cpu().numpy()
+    np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-5 * np.abs(ref).max())
+    gotp = _kernels.frames("power", xt, wt, N, N, hop, code, False).cpu().numpy()
+    refp = np.abs(np.fft.fft(fr * win.astype(np.float64), axis=-1)) ** 2
+    np.testing.assert_allclose(gotp, refp, rtol=1e-4, atol=1e-5 * refp.max())
+
+
+ISTFT_CASES = [
+    {},
+    {"boundary": False},
+    {"scaling": "psd"},
+    {"nperseg": 256, "noverlap": 192},
+    {"window": "hamming"},
+]
+
+
+@pytest.mark.parametrize("case", ISTFT_CASES)
+def test_istft_matches_scipy(rng, case):
+    x = make_sig(rng, (4000,))
+    stft_kw = {k: case[k] for k in ("nperseg", "noverlap", "window") if k in case}
+    if case.get("scaling") == "psd":
+        stft_kw["scaling"] = "psd"
+    if case.get("boundary") is False:
+        stft_kw["boundary"] = None
+    f, t, z = sps.stft(x.astype(np.float64), **stft_kw)
+    if case.get("boundary") is False:
+        import warnings as _w
+
+        with _w.catch_warnings():
+            _w.simplefilter("ignore")
+            t_ref, x_ref = sps.istft(z, **case)
+            t2, x2 = msig.istft(z, **case)
+        assert x_ref.shape == tuple(x2.shape)
+        assert_close(x2.cpu().numpy()[128:-128], x_ref[128:-128])
+    else:
+        t_ref, x_ref = sps.istft(z, **case)
+        t2, x2 = msig.istft(z, **case)
+        assert x_ref.shape == tuple(x2.shape)
+        assert_close(x2, x_ref)
+    assert_close(t2, t_ref)
+
+
+def test_istft_twosided(rng):
+    x = make_sig(rng, (2048,))
+    _, _, z = sps.stft(x.astype(np.float64), return_onesided=False)
+    t_ref, x_ref = sps.istft(z, input_onesided=False)
+    t2, x2 = msig.istft(z, input_onesided=False)
+    assert_close(x2.real if x2.is_complex() else x2, x_ref.real)
+
+
+def test_istft_batched(rng):
+    x = make_sig(rng, (3, 4000))
+    _, _, z = sps.stft(x.astype(np.float64))
+    t_ref, x_ref = sps.istft(z)
+    t2, x2 = msig.istft(z)
+    assert x_ref.shape == tuple(x2.shape)
+    assert_close(x2, x_ref)
+
+
+@pytest.mark.parametrize(
+    "perm,freq_axis,time_axis",
+    [((0, 1, 2, 3), -2, -1), ((0, 1, 3, 2), -1, -2), ((2, 0, 1, 3), 0, -1), ((2, 3, 0, 1), 0, 1),
+     ((3, 2, 0, 1), 1, 0), ((0, 3, 1, 2), 3, 1), ((0, 2, 3, 1), 1, 2), ((0, 3, 2, 1), 2, 1)],
+)
+@pytest.mark.parametrize("nperseg", [256, 200])
+def test_istft_arbitrary_axes(rng, perm, freq_axis, time_axis, nperseg):
+    x = make_sig(rng, (2, 3, 1024))
+    _, _, z = sps.stft(x.astype(np.float64), nperseg=nperseg)
+    z = np.transpose(z.astype(np.complex64), perm)
+    _, x_ref = sps.istft(z, nperseg=nperseg, freq_axis=freq_axis, time_axis=time_axis)
+    t_got, x_got = msig.istft(z, nperseg=nperseg, freq_axis=freq_axis, time_axis=time_axis)
+    assert tuple(x_got.shape) == x_ref.shape
+    out_time_ax = (time_axis % z.ndim) - (1 if (freq_axis % z.ndim) < (time_axis % z.ndim) else 0)
+    assert len(t_got) == x_got.shape[out_time_ax]
+    assert_close(x_got, x_ref)
+
+
+def test_istft_axis_and_dtype_validation(rng):
+    x = make_sig(rng, (2, 1024))
+    _, _, z = sps.stft(x, nperseg=128)
+    z = z.astype(np.complex64)
+    with pytest.raises(ValueError, match="at least 2d"):
+        msig.istft(np.ones(16, dtype=np.complex64))
+    with pytest.raises(ValueError, match="differing"):
+        msig.istft(z, freq_axis=-1, time_axis=-1)
+    with pytest.raises(ValueError, match="differing"):
+        msig.istft(z, freq_axis=1, time_axis=-2)
+    with pytest.raises(IndexError):
+        msig.istft(z, freq_axis=5, time_axis=-1)
+    z128 = z.astype(np.complex128)
+    with msig.config_context(float64="strict"):
+        with pytest.raises(TypeError, match="strict"):
+            msig.istft(z128, nperseg=128)
+    with msig.config_context(float64="downcast", warn_on_downcast=True):
+        with pytest.warns(msig.DowncastWarning):
+            msig.istft(z128, nperseg=128)
+
+
+def test_stft_istft_roundtrip_ours(rng):
+    x = make_sig(rng, (4096,))
+    f, t, z = msig.stft(x, nperseg=256)
+    t2, x2 = msig.istft(z, nperseg=256)
+    x2 = x2.cpu().numpy()[: len(x)]
+    np.testing.assert_allclose(x2, x, rtol=1e-4, atol=1e-4)

@@ -1,0 +1,228 @@
+"""GPU parity: welch / periodogram / csd / coherence against float64 scipy.signal.
+
+Cases follow the reference's tests/test_spectral.py (WELCH_CASES, multidim axes, csd
+mean/median/broadcast/unequal, coherence, grouped-vs-scipy over nperseg 64..2048) and add the
+north-star accuracy bar (max relative error <= 1e-5 on bins above 1e-6 of the peak).
+"""
+
+import numpy as np
+import pytest
+import scipy.signal as sps
+import torch
+
+import mlx_signal_b200 as msig
+from _utils import assert_close, assert_cuda_f32, make_sig, rel_err_bins
+
+pytestmark = pytest.mark.gpu
+
+WELCH_CASES = [
+    {},
+    {"nperseg": 128},
+    {"nperseg": 128, "noverlap": 96},
+    {"nperseg": 128, "window": "hamming"},
+    {"nperseg": 100, "window": ("tukey", 0.25)},
+    {"nperseg": 128, "detrend": "linear"},
+    {"nperseg": 128, "detrend": False},
+    {"nperseg": 128, "scaling": "spectrum"},
+    {"nperseg": 128, "return_onesided": False},
+    {"nperseg": 128, "average": "median"},
+    {"nperseg": 128, "nfft": 256},
+    {"nperseg": 129, "noverlap": 37, "fs": 250.0},
+]
+
+
+@pytest.mark.parametrize("n", [1024, 999, 4093])
+@pytest.mark.parametrize("case", WELCH_CASES)
+def test_welch_matches_scipy(rng, n, case):
+    x = make_sig(rng, (n,))
+    f_ref, p_ref = sps.welch(x.astype(np.float64), **case)
+    f, p = msig.welch(x, **case)
+    assert_cuda_f32(f)
+    assert_cuda_f32(p)
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+
+
+def test_welch_array_window(rng):
+    x = make_sig(rng, (2048,))
+    w = sps.get_window("hann", 200)
+    f_ref, p_ref = sps.welch(x.astype(np.float64), window=w)
+    f, p = msig.welch(x, window=w.astype(np.float32))
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+
+
+@pytest.mark.parametrize(
+    "shape,axis", [((3, 2000), -1), ((2000, 3), 0), ((2, 3, 1500), -1), ((2, 1500, 3), 1)]
+)
+def test_welch_multidim(rng, shape, axis):
+    x = make_sig(rng, shape)
+    f_ref, p_ref = sps.welch(x.astype(np.float64), nperseg=128, axis=axis)
+    f, p = msig.welch(x, nperseg=128, axis=axis)
+    assert p_ref.shape == tuple(p.shape)
+    assert_close(p, p_ref)
+    assert_close(f, f_ref)
+
+
+def test_welch_complex_input_switches_twosided(rng):
+    x = make_sig(rng, (2048,), complex_=True)
+    f_ref, p_ref = sps.welch(x.astype(np.complex128), nperseg=256)
+    f, p = msig.welch(x, nperseg=256)
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+
+
+def test_welch_short_signal_warns(rng):
+    x = make_sig(rng, (100,))
+    with pytest.warns(UserWarning, match="nperseg"):
+        f_ref, p_ref = sps.welch(x.astype(np.float64))
+    with pytest.warns(UserWarning, match="nperseg"):
+        f, p = msig.welch(x)
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+
+
+@pytest.mark.parametrize(
+    "case",
+    [{}, {"nfft": 4096}, {"nfft": 1000}, {"scaling": "spectrum"}, {"detrend": False},
+     {"window": "hann"}, {"return_onesided": False}],
+)
+def test_periodogram_matches_scipy(rng, case):
+    x = make_sig(rng, (2048,))
+    f_ref, p_ref = sps.periodogram(x.astype(np.float64), **case)
+    f, p = msig.periodogram(x, **case)
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+
+
+def test_parseval_periodogram(rng):
+    x = make_sig(rng, (4096,))
+    fs = 10.0
+    f, p = msig.periodogram(x, fs=fs, detrend=False)
+    total = float(p.double().sum().item()) * fs / len(x)
+    np.testing.assert_allclose(total, np.mean(x.astype(np.float64) ** 2), rtol=1e-3)
+
+
+@pytest.mark.parametrize("average", ["mean", "median"])
+def test_csd_matches_scipy(rng, average):
+    x = make_sig(rng, (4096,))
+    y = make_sig(rng, (4096,))
+    f_ref, p_ref = sps.csd(x.astype(np.float64), y.astype(np.float64), nperseg=256,
+                           average=average)
+    f, p = msig.csd(x, y, nperseg=256, average=average)
+    assert p.dtype == torch.complex64
+    assert_close(f, f_ref)
+    assert_close(p, p_ref, rtol=2e-4)
+
+
+def test_csd_broadcast(rng):
+    x = make_sig(rng, (4096,))
+    y = make_sig(rng, (3, 4096))
+    f_ref, p_ref = sps.csd(x.astype(np.float64), y.astype(np.float64), nperseg=256)
+    f, p = msig.csd(x, y, nperseg=256)
+    assert p_ref.shape == tuple(p.shape)
+    assert_close(p, p_ref, rtol=2e-4)
+
+
+def test_csd_unequal_lengths(rng):
+    x = make_sig(rng, (3000,))
+    y = make_sig(rng, (4096,))
+    f_ref, p_ref = sps.csd(x.astype(np.float64), y.astype(np.float64), nperseg=256)
+    f, p = msig.csd(x, y, nperseg=256)
+    assert_close(p, p_ref, rtol=2e-4)
+
+
+def test_coherence_matches_scipy(rng):
+    x = make_sig(rng, (8192,))
+    y = 0.5 * x + 0.5 * make_sig(rng, (8192,))
+    f_ref, c_ref = sps.coherence(x.astype(np.float64), y.astype(np.float64), nperseg=256)
+    f, c = msig.coherence(x, y, nperseg=256)
+    assert_close(c, c_ref, rtol=1e-3)
+    assert float(c.min()) >= 0.0 and float(c.max()) <= 1.0
+
+
+@pytest.mark.parametrize("nperseg", [64, 128, 256, 512, 1024, 2048])
+@pytest.mark.parametrize("detrend", [False, "constant"])
+def test_grouped_spectral_means_match_scipy(rng, nperseg, detrend):
+    n = nperseg + (nperseg // 2) * 130
+    x = make_sig(rng, (16, n))
+    y = (0.5 * x + 0.5 * make_sig(rng, (16, n))).astype(np.float32)
+    x64, y64 = x.astype(np.float64), y.astype(np.float64)
+    _, pw = msig.welch(x, nperseg=nperseg, detrend=detrend)
+    _, pw_ref = sps.welch(x64, nperseg=nperseg, detrend=detrend)
+    assert_close(pw, pw_ref, rtol=1e-4)
+    assert rel_err_bins(pw, pw_ref) < 1e-5
+    _, pc = msig.csd(x, y, nperseg=nperseg, detrend=detrend)
+    _, pc_ref = sps.csd(x64, y64, nperseg=nperseg, detrend=detrend)
+    assert_close(pc, pc_ref, rtol=2e-4)
+    _, co = msig.coherence(x, y, nperseg=nperseg, detrend=detrend)
+    _, co_ref = sps.coherence(x64, y64, nperseg=nperseg, detrend=detrend)
+    assert_close(co, co_ref, rtol=1e-3)
+
+
+def test_grouped_single_group_and_nonlast_axis(rng):
+    x_many = make_sig(rng, (2048, 320))
+    y_many = (0.5 * x_many + 0.5 * make_sig(rng, (2048, 320))).astype(np.float32)
+    assert_close(msig.welch(x_many, nperseg=64)[1],
+                 sps.welch(x_many.astype(np.float64), nperseg=64)[1], rtol=1e-4)
+    assert_close(msig.coherence(x_many, y_many, nperseg=64)[1],
+                 sps.coherence(x_many.astype(np.float64), y_many.astype(np.float64),
+                               nperseg=64)[1], rtol=1e-3)
+    x_ax = make_sig(rng, (2, 4096, 3))
+    y_ax = (0.5 * x_ax + 0.5 * make_sig(rng, (2, 4096, 3))).astype(np.float32)
+    x64, y64 = x_ax.astype(np.float64), y_ax.astype(np.float64)
+    assert_close(msig.welch(x_ax, nperseg=128, axis=1)[1],
+                 sps.welch(x64, nperseg=128, axis=1)[1], rtol=1e-4)
+    assert_close(msig.csd(x_ax, y_ax, nperseg=128, axis=1)[1],
+                 sps.csd(x64, y64, nperseg=128, axis=1)[1], rtol=2e-4)
+    assert_close(msig.coherence(x_ax, y_ax, nperseg=128, axis=1)[1],
+                 sps.coherence(x64, y64, nperseg=128, axis=1)[1], rtol=1e-3)
+
+
+@pytest.mark.parametrize("nfft", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096])
+@pytest.mark.parametrize("detrend", [False, "constant", "linear"])
+def test_fused_welch_every_size(rng, nfft, detrend):
+    """Every fused team-FFT plan (single-thread up to 32 points, 8..128-thread teams above),
+    with nperseg < nfft zero padding and an odd hop."""
+    nperseg = max(1, nfft - nfft // 4)
+    hop = max(1, nperseg // 2 - 1) if nperseg > 2 else 1
+    x = make_sig(rng, (3, 40 * nfft + 7))
+    kw = dict(nperseg=nperseg, noverlap=nperseg - hop, nfft=nfft, detrend=detrend)
+    # an absolute floor at the signal power: degenerate cases (linear detrend of 1-2 samples)
+    # are exactly zero in float64 and fp32 rounding noise here
+    floor = 1e-5 * float(np.mean(x.astype(np.float64) ** 2))
+    _, p = msig.welch(x, **kw)
+    _, p_ref = sps.welch(x.astype(np.float64), **kw)
+    np.testing.assert_allclose(p.cpu().numpy(), p_ref, rtol=1e-4,
+                               atol=max(1e-5 * np.abs(p_ref).max(), floor))
+    _, c = msig.csd(x, x[::-1].copy(), **kw)
+    _, c_ref = sps.csd(x.astype(np.float64), x[::-1].astype(np.float64), **kw)
+    np.testing.assert_allclose(c.cpu().numpy(), c_ref, rtol=2e-4,
+                               atol=max(2e-5 * np.abs(c_ref).max(), floor))
+
+
+def test_welch_north_star_accuracy(rng):
+    """48 kHz multi-tone channels, hann, nperseg 1024 / 50%: <= 1e-5 relative on bins above
+    1e-6 of the peak (scaled-down channel count of the 64 x 2^20 workload)."""
+    fs = 48000.0
+    C, n = 8, 1 << 18
+    t = np.arange(n) / fs
+    x = rng.standard_normal((C, n))
+    for c in range(C):
+        for _ in range(rng.integers(1, 5)):
+            x[c] += rng.uniform(0.1, 2.0) * np.sin(2 * np.pi * rng.uniform(0, fs / 2) * t)
+    x = x.astype(np.float32)
+    _, p = msig.welch(x, fs=fs, nperseg=1024, noverlap=512)
+    _, p_ref = sps.welch(x.astype(np.float64), fs=fs, nperseg=1024, noverlap=512)
+    err = max(rel_err_bins(p[c], p_ref[c]) for c in range(C))
+    assert err <= 1e-5, err
+
+
+def test_torch_inputs_and_outputs(rng):
+    x = make_sig(rng, (4, 8192))
+    xt = torch.from_numpy(x).cuda()
+    f1, p1 = msig.welch(x, nperseg=512)
+    f2, p2 = msig.welch(xt, nperseg=512)
+    torch.testing.assert_close(p1, p2, rtol=0, atol=0)
+    f3, p3 = msig.welch(torch.from_numpy(x), nperseg=512)
+    torch.testing.assert_close(p1, p3, rtol=0, atol=0)
