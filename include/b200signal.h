@@ -72,6 +72,22 @@ SP_API int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, con
                  void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * sp_welch_f32 without a workspace argument, for callers that cannot allocate device memory
+ * (plugin hosts that only receive input/output pointers, latency-critical loops that must not
+ * call cudaMalloc after start-up). No counterpart in the reference: it is an addition of this
+ * library. The partial sums live in a fixed 16 MiB static device array that every GPU loading
+ * the library holds until exit; shapes needing more scratch than that return SP_ERR_WORKSPACE
+ * (sp_mean_workspace_size(0, ...) gives the need). It calls no cudaMalloc/cudaFree. The first
+ * call on a device resolves the array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture. All calls share the one array: calls that overlap on the GPU (for
+ * example on two streams at once) race and must be serialised by the caller. Nothing from a
+ * previous call is read: every partial sum a call reads is written by that call first.
+ */
+SP_API int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld,
+                                const float* win, int nperseg, int nfft, int hop, int detrend,
+                                int onesided, float* out, void* stream);
+
+/*
  * Cross spectral density mean conj(X_s) Y_s over segments (complex64 out, same bin count and
  * one-sided doubling as sp_welch_f32). Replaces _stft_metal.csd_mean (_stft_metal.py:739-741).
  */

@@ -1,4 +1,5 @@
 // C-ABI: segment-mean spectral estimates (welch / csd / coherence).
+#include <mutex>
 #include <utility>
 
 #include "capi_common.h"
@@ -166,10 +167,66 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   return SP_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Fixed scratch for sp_welch_f32_noalloc. Some callers cannot allocate device memory at call
+// time: plugin hosts that only hand over input/output pointers owned by another framework, and
+// latency-critical loops that must not take cudaMalloc's implicit device synchronisation or
+// grow their footprint after start-up. For them the partial-sum workspace lives in this
+// file-scope array. It is created when the library's module is loaded on a device and stays
+// allocated on every GPU that loads the library until the process exits.
+// ---------------------------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device. In host code the array's name is
+// only a host-side stand-in, so the address comes from cudaGetSymbolAddress, once per device
+// (with that device current), and is cached.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  B2S_CHECK_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_error("sp_welch_f32_noalloc: device index %d beyond the supported %d", dev,
+              kNoAllocMaxDevices);
+    return SP_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* p = nullptr;
+    B2S_CHECK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return SP_OK;
+}
+
 }  // namespace
 }  // namespace b2s
 
 extern "C" {
+
+int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
+                         int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
+                         void* stream) {
+  b2s::MeanPlanInfo pl;
+  const int st = b2s::make_plan(false, rows, n, nperseg, nfft, hop, detrend, &pl);
+  if (st != SP_OK) return st;
+  if (size_t(pl.ws_bytes) > b2s::kNoAllocScratchBytes) {
+    b2s::set_error(
+        "sp_welch_f32_noalloc: this shape needs %lld bytes of scratch but the built-in scratch "
+        "holds %zu bytes; use sp_welch_f32 with a caller-provided workspace",
+        (long long)pl.ws_bytes, b2s::kNoAllocScratchBytes);
+    return SP_ERR_WORKSPACE;
+  }
+  void* ws = nullptr;
+  const int sst = b2s::noalloc_scratch(&ws);
+  if (sst != SP_OK) return sst;
+  return b2s::run_mean(0, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, onesided,
+                       out, ws, b2s::kNoAllocScratchBytes, stream);
+}
 
 int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
                                int detrend) {
