@@ -1,0 +1,91 @@
+"""CPU: host-side argument logic that runs before any device call (no GPU needed)."""
+
+import numpy as np
+import pytest
+
+import mlx_signal_b200 as msig
+from mlx_signal_b200 import _kernels, spectral
+from mlx_signal_b200.windows import ByteBudgetCache, _window_np
+
+
+def test_triage_string_window_and_short_signal_warning():
+    with pytest.warns(UserWarning, match="nperseg"):
+        w, n = spectral._triage_segments("hann", 512, input_length=100)
+    assert n == 100 and w.shape == (100,)
+    w, n = spectral._triage_segments(("tukey", 0.25), None, input_length=1000)
+    assert n == 256
+
+
+def test_triage_array_window_errors():
+    with pytest.raises(ValueError, match="1-D"):
+        spectral._triage_segments(np.ones((2, 2)), None, 100)
+    with pytest.raises(ValueError, match="longer than input"):
+        spectral._triage_segments(np.ones(200), None, 100)
+    with pytest.raises(ValueError, match="different from length of window"):
+        spectral._triage_segments(np.ones(64), 32, 100)
+
+
+def test_detrend_codes():
+    assert spectral._detrend_code(False) == 0
+    assert spectral._detrend_code("constant") == 1
+    assert spectral._detrend_code("l") == 2
+    with pytest.raises(ValueError, match="Trend type"):
+        spectral._detrend_code("quadratic")
+    with pytest.raises(NotImplementedError):
+        spectral._detrend_code(lambda d: d)
+
+
+def test_istft_axes_validation():
+    assert spectral._istft_axes((2, 3, 129, 40), -2, -1) == (2, 3, [0, 1, 3, 2])
+    with pytest.raises(ValueError, match="at least 2d"):
+        spectral._istft_axes((16,), -2, -1)
+    with pytest.raises(ValueError, match="differing"):
+        spectral._istft_axes((4, 5), 1, -1)
+    with pytest.raises(IndexError):
+        spectral._istft_axes((4, 5), 5, -1)
+
+
+def test_onesided_factor_and_median_bias():
+    f = spectral._onesided_factor_np(8)
+    assert f.tolist() == [1, 2, 2, 2, 1]
+    assert spectral._onesided_factor_np(7).tolist() == [1, 2, 2, 2]
+    assert spectral._median_bias(1) == 1.0
+    assert abs(spectral._median_bias(5) - (1 + 1 / 3 - 1 / 2 + 1 / 5 - 1 / 4)) < 1e-15
+
+
+def test_fused_routing_rule():
+    assert _kernels.fused_mean_ok(1024) and _kernels.fused_mean_ok(1)
+    assert not _kernels.fused_mean_ok(100) and not _kernels.fused_mean_ok(8192)
+
+
+def test_config_validation_and_context():
+    with pytest.raises(ValueError, match="no CPU"):
+        msig.set_config(dispatch="scipy")
+    with pytest.raises(TypeError):
+        msig.set_config(nonsense=1)
+    base = msig.get_config().float64
+    with msig.config_context(float64="strict"):
+        assert msig.get_config().float64 == "strict"
+    assert msig.get_config().float64 == base
+
+
+def test_dtype_policy_without_device():
+    from mlx_signal_b200 import _array
+
+    with msig.config_context(float64="strict"):
+        with pytest.raises(TypeError, match="strict"):
+            _array.check_dtype_policy(np.zeros(4))
+    with msig.config_context(float64="downcast", warn_on_downcast=True):
+        with pytest.warns(msig.DowncastWarning):
+            _array.check_dtype_policy(np.zeros(4, dtype=np.complex128))
+
+
+def test_window_cache_and_byte_budget():
+    w = _window_np("hann", 64)
+    assert w.dtype == np.float64 and not w.flags.writeable
+    c = ByteBudgetCache(100)
+    c.put(("a",), 1, 60)
+    c.put(("b",), 2, 60)
+    assert c.get(("a",)) is None and c.get(("b",)) == 2
+    c.put(("huge",), 3, 1000)
+    assert c.get(("huge",)) is None
