@@ -72,6 +72,26 @@ SP_API int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, con
                  void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * sp_welch_f32 with the constant detrend applied in the frequency domain. `win_dft_low` is a
+ * device pointer to n_low complex64 values DFT_nfft(win)[0..n_low) (win zero-padded to nfft);
+ * the caller guarantees that DFT_nfft(win)[k] is zero (to float32 rounding) for
+ * n_low <= k <= nfft - n_low, as for hann / hamming / blackman / boxcar. The segment means are
+ * then removed as Z_k -= m * DFT(win)_k on those bins only, off the FFT's critical path. Used
+ * when detrend == SP_DETREND_CONSTANT, nperseg == nfft == 2*hop and
+ * 1 <= n_low <= sp_welch_spectral_bins(nfft); otherwise identical to sp_welch_f32 (pass NULL).
+ * Same reference counterpart as sp_welch_f32 (_stft_metal.py:530-557; the reference subtracts
+ * the mean in the time domain, _stft_metal.py:40-61).
+ */
+SP_API int sp_welch_f32_ex(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
+                           const float* win_dft_low, int n_low, int nperseg, int nfft, int hop,
+                           int detrend, int onesided, float* out, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* Largest n_low sp_welch_f32_ex accepts for this nfft (0 if nfft is not a supported power of
+ * two). */
+SP_API int sp_welch_spectral_bins(int nfft);
+
+/*
  * sp_welch_f32 without a workspace argument, for callers that cannot allocate device memory
  * (plugin hosts that only receive input/output pointers, latency-critical loops that must not
  * call cudaMalloc after start-up). No counterpart in the reference: it is an addition of this

@@ -8,6 +8,7 @@ csd_mean :739, coherence_mean :744).
 
 from __future__ import annotations
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -41,8 +42,12 @@ def _workspace(nbytes: int, dev: torch.device) -> torch.Tensor:
 
 
 def welch_mean(x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop: int,
-               detrend: int, onesided: bool) -> torch.Tensor:
-    """Mean |FFT(win * detrend(segment))|^2 over segments of each row of x -> (rows, nout)."""
+               detrend: int, onesided: bool, wdft: torch.Tensor | None = None) -> torch.Tensor:
+    """Mean |FFT(win * detrend(segment))|^2 over segments of each row of x -> (rows, nout).
+
+    `wdft` (optional, complex64 CUDA): the non-zero low bins DFT_nfft(win)[0..n_low) of a window
+    whose spectrum vanishes elsewhere; lets the constant detrend run as a spectral correction.
+    """
     x, ld = _rows(x)
     rows, n = x.shape
     lib = _lib.load()
@@ -52,6 +57,14 @@ def welch_mean(x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop:
     nout = nfft // 2 + 1 if onesided else nfft
     out = torch.empty((rows, nout), dtype=torch.float32, device=x.device)
     ws = _workspace(ws_bytes, x.device)
+    if wdft is not None:
+        _lib.check(
+            lib.sp_welch_f32_ex(x.data_ptr(), rows, n, ld, win.data_ptr(), wdft.data_ptr(),
+                                wdft.numel(), nperseg, nfft, hop, detrend, int(onesided),
+                                out.data_ptr(), ws.data_ptr(), ws.numel(), stream_handle()),
+            "sp_welch_f32_ex",
+        )
+        return out
     _lib.check(
         lib.sp_welch_f32(x.data_ptr(), rows, n, ld, win.data_ptr(), nperseg, nfft, hop, detrend,
                          int(onesided), out.data_ptr(), ws.data_ptr(), ws.numel(),
@@ -59,6 +72,24 @@ def welch_mean(x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop:
         "sp_welch_f32",
     )
     return out
+
+
+def window_low_spectrum(win32, nfft: int):
+    """(DFT_nfft(win)[0..n_low) as complex64 numpy, n_low) when the window's spectrum is
+    non-zero only on |k| < n_low (mod nfft) and n_low fits the kernel's spectral-detrend
+    bins; else None. `win32` are the float32 window values the kernel multiplies by."""
+    if not is_pow2(nfft) or nfft < 2:
+        return None
+    wf = np.fft.fft(np.asarray(win32, dtype=np.float64), n=nfft)
+    mag = np.abs(wf)
+    peak = mag.max()
+    if peak == 0.0:
+        return None
+    k = np.nonzero(mag > 1e-7 * peak)[0]
+    n_low = int(np.max(np.minimum(k, nfft - k))) + 1
+    if n_low > _lib.load().sp_welch_spectral_bins(nfft):
+        return None
+    return wf[:n_low].astype(np.complex64), n_low
 
 
 def cross_mean(mode: str, x: torch.Tensor, y: torch.Tensor, win: torch.Tensor, nperseg: int,

@@ -11,7 +11,7 @@
 #include <string>
 #include <unordered_map>
 
-#include "../../include/b200signal.h"
+#include "b200signal.h"
 
 namespace b2s {
 

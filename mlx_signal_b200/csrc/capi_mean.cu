@@ -13,6 +13,7 @@ constexpr int kMaxLog = kMaxLogL;
 }  // namespace
 
 __global__ void k_reduce_mean(ReduceParams p) {
+  pdl_wait();  // launched as a programmatic dependent of the segment kernel
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= p.rows * p.nout) return;
   const int64_t r = idx / p.nout;
@@ -27,13 +28,16 @@ __global__ void k_reduce_mean(ReduceParams p) {
   double fac = 1.0 / double(p.nseg);
   if (p.onesided && k != 0 && 2 * k != L) fac *= 2.0;
   if (p.mode == 0) {
-    const float* base = p.partial + r * p.cmax * int64_t(L);
-    double s = 0.0;
-    for (int c = 0; c < nsl; ++c) {
-      const float* q = base + int64_t(c) * L;
-      s += double(q[k]) + double(q[kk]);
+    const int stride = welch_slot_floats(L);
+    const float* q = p.partial + r * p.cmax * int64_t(stride) + kc;
+    double s0 = 0.0, s1 = 0.0;
+    int c = 0;
+    for (; c + 1 < nsl; c += 2) {
+      s0 += double(q[int64_t(c) * stride]);
+      s1 += double(q[int64_t(c + 1) * stride]);
     }
-    p.out[idx] = float(0.5 * s * fac);
+    if (c < nsl) s0 += double(q[int64_t(c) * stride]);
+    p.out[idx] = float(0.5 * (s0 + s1) * fac);
     return;
   }
   const int stride = cross_slot_floats(L);
@@ -76,8 +80,12 @@ struct MeanPlanInfo {
   int64_t ws_bytes = 0;
 };
 
+// Largest count of low window-spectrum bins the spectral detrend correction can apply: the
+// bins k < P and k > L - P are the first and last register of every team thread.
+int spectral_bins(int log_l) { return (1 << log_l) >> team_log_e_rt(log_l); }
+
 int make_plan(bool cross, int64_t rows, int64_t n, int nperseg, int nfft, int hop, int detrend,
-              MeanPlanInfo* pl) {
+              MeanPlanInfo* pl, bool spectral = false) {
   if (rows < 0 || n < 1 || nperseg < 1 || nperseg > n || hop < 1 || hop > nperseg ||
       nfft < nperseg || detrend < 0 || detrend > 2 || n >= (int64_t(1) << 31)) {
     set_error("invalid spectral-mean arguments (rows=%lld n=%lld nperseg=%d nfft=%d hop=%d)",
@@ -89,7 +97,10 @@ int make_plan(bool cross, int64_t rows, int64_t n, int nperseg, int nfft, int ho
     set_error("nfft=%d: fused kernels need a power of two <= %d", nfft, 1 << kMaxLog);
     return SP_ERR_UNSUPPORTED;
   }
-  pl->k = cross ? mean_lookup_cross(log_l, detrend) : mean_lookup_welch(log_l, detrend);
+  const bool half = !cross && log_l >= 1 && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
+  pl->k = cross ? mean_lookup_cross(log_l, detrend)
+                : (half ? mean_lookup_welch_half(log_l, (spectral && detrend == 1) ? 2 : detrend)
+                        : mean_lookup_welch(log_l, detrend));
   pl->log_l = log_l;
   pl->nseg = int((n - nperseg) / hop + 1);
   pl->total = rows * pl->nseg;
@@ -109,21 +120,25 @@ int make_plan(bool cross, int64_t rows, int64_t n, int nperseg, int nfft, int ho
   if (cm > pl->nteams) cm = pl->nteams;
   pl->cmax = int(cm);
   const int64_t L = int64_t(1) << log_l;
-  pl->slot_floats = cross ? cross_slot_floats(int(L)) : L;
+  pl->slot_floats = cross ? cross_slot_floats(int(L)) : welch_slot_floats(int(L));
   pl->ws_bytes = rows * pl->cmax * pl->slot_floats * int64_t(sizeof(float));
   return SP_OK;
 }
 
 int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
              int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
-             int onesided, float* out, void* ws, size_t ws_bytes, void* stream) {
+             int onesided, float* out, void* ws, size_t ws_bytes, void* stream,
+             const float* wdft = nullptr, int n_low = 0) {
   const bool cross = mode != 0;
   if (!x || !win || !out || (cross && !y) || ldx < n || (cross && ldy < n)) {
     set_error("null pointer or row stride smaller than n");
     return SP_ERR_ARG;
   }
+  const int log_l_in = ilog2_exact(nfft);
+  const bool spectral = !cross && wdft != nullptr && n_low >= 1 && log_l_in >= 1 &&
+                        n_low <= spectral_bins(log_l_in);
   MeanPlanInfo pl;
-  int st = make_plan(cross, rows, n, nperseg, nfft, hop, detrend, &pl);
+  int st = make_plan(cross, rows, n, nperseg, nfft, hop, detrend, &pl, spectral);
   if (st != SP_OK) return st;
   if (rows == 0) return SP_OK;
   if (ws_bytes < size_t(pl.ws_bytes) || (pl.ws_bytes > 0 && !ws)) {
@@ -146,6 +161,8 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   p.cmax = pl.cmax;
   p.total = pl.total;
   p.partial = static_cast<float*>(ws);
+  p.wdft = spectral ? reinterpret_cast<const float2*>(wdft) : nullptr;
+  p.n_low = spectral ? n_low : 0;
   pl.k.launch(dim3(unsigned(pl.blocks)), pl.k.threads, pl.k.smem, s, p);
   B2S_CHECK_CUDA(cudaGetLastError(), "spectral-mean kernel launch");
   ReduceParams rp;
@@ -161,9 +178,18 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   rp.mode = mode;
   rp.out = out;
   const int64_t nthr = rows * rp.nout;
-  const int tb = 256;
-  k_reduce_mean<<<unsigned(cdiv(nthr, tb)), tb, 0, s>>>(rp);
-  B2S_CHECK_CUDA(cudaGetLastError(), "spectral-mean reduce launch");
+  const int tb = 128;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(cdiv(nthr, tb)));
+  cfg.blockDim = dim3(tb);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  B2S_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_reduce_mean, rp), "spectral-mean reduce launch");
   return SP_OK;
 }
 
@@ -240,6 +266,20 @@ int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, const floa
                  void* workspace, size_t workspace_bytes, void* stream) {
   return b2s::run_mean(0, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, onesided,
                        out, workspace, workspace_bytes, stream);
+}
+
+int sp_welch_spectral_bins(int nfft) {
+  const int log_l = b2s::ilog2_exact(nfft);
+  if (log_l < 1 || log_l > b2s::kMaxLog) return 0;
+  return b2s::spectral_bins(log_l);
+}
+
+int sp_welch_f32_ex(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
+                    const float* win_dft_low, int n_low, int nperseg, int nfft, int hop,
+                    int detrend, int onesided, float* out, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(0, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, onesided,
+                       out, workspace, workspace_bytes, stream, win_dft_low, n_low);
 }
 
 int sp_csd_c64(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,

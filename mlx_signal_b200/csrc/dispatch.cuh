@@ -20,6 +20,11 @@ constexpr int team_log_e() {
 
 constexpr int kMaxLogL = 12;
 
+// Runtime twin of team_log_e.
+inline int team_log_e_rt(int log_l) {
+  return log_l <= 5 ? log_l : (log_l == 6 ? 3 : (log_l <= 8 ? 4 : 5));
+}
+
 template <class P>
 using LaunchFnT = void (*)(dim3, int, size_t, cudaStream_t, const P&);
 
@@ -38,6 +43,7 @@ using FrameInfo = KernelInfo<FrameParams>;
 // family: 0 welch mean, 1 cross mean
 MeanInfo mean_lookup_welch(int log_l, int det);
 MeanInfo mean_lookup_cross(int log_l, int det);
+MeanInfo mean_lookup_welch_half(int log_l, int det);  // det 0/1/2(spectral), log_l >= 1
 FrameInfo frame_lookup_stft(int log_l, int det);
 FrameInfo frame_lookup_power(int log_l, int det);
 FrameInfo frame_lookup_cross(int log_l, int det);

@@ -20,6 +20,8 @@ struct MeanParams {
   int cmax;            // partial-sum slots per row
   int64_t total;       // rows * nseg
   float* partial;      // workspace: [rows][cmax][slot_floats]
+  const float2* wdft;  // DFT_L(win)[0..n_low) for the spectral detrend correction, else nullptr
+  int n_low;           // bins of the window spectrum that are non-zero: |k| < n_low (mod L)
 };
 
 // Per-frame kernels (stft / spectrogram / per-frame cross spectra).

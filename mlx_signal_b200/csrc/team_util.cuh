@@ -52,6 +52,30 @@ __device__ __forceinline__ float4 team_sum4(float4 v, float4* scratch, unsigned 
   }
 }
 
+// Sum NV floats (in place) across the P threads of a team; same layout rules as team_sum4.
+template <int P, int NV>
+__device__ __forceinline__ void team_sum(float (&v)[NV], float4* scratch, unsigned mask) {
+  static_assert(NV <= 4, "at most four values per reduction");
+  if constexpr (P <= 32) {
+#pragma unroll
+    for (int off = P / 2; off > 0; off >>= 1) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) v[i] += __shfl_xor_sync(mask, v[i], off);
+    }
+  } else {
+    float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (NV > 0) f.x = v[0];
+    if constexpr (NV > 1) f.y = v[1];
+    if constexpr (NV > 2) f.z = v[2];
+    if constexpr (NV > 3) f.w = v[3];
+    f = team_sum4<P>(f, scratch, mask);
+    if constexpr (NV > 0) v[0] = f.x;
+    if constexpr (NV > 1) v[1] = f.y;
+    if constexpr (NV > 2) v[2] = f.z;
+    if constexpr (NV > 3) v[3] = f.w;
+  }
+}
+
 // Lane mask of the team containing this thread (teams of P <= 32 lanes are aligned groups).
 template <int P>
 __device__ __forceinline__ unsigned team_mask() {
@@ -63,8 +87,15 @@ __device__ __forceinline__ unsigned team_mask() {
   }
 }
 
-// Detrend kinds (scipy.signal.detrend semantics per segment).
-enum : int { kDetrendNone = 0, kDetrendConstant = 1, kDetrendLinear = 2 };
+// Detrend kinds (scipy.signal.detrend semantics per segment). kDetrendConstantSpectral is the
+// constant detrend applied after the FFT as Z_k -= m * DFT(win)_k, valid when the window's DFT
+// vanishes outside a few low bins (hann, hamming, blackman, boxcar, ...).
+enum : int {
+  kDetrendNone = 0,
+  kDetrendConstant = 1,
+  kDetrendLinear = 2,
+  kDetrendConstantSpectral = 3
+};
 
 // Element index of register slot `slot` in the pass-0 load pattern: slot = b*R0 + bitrev(q)
 // holds element t + P*b + q*(L/R0).

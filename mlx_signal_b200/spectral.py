@@ -280,6 +280,26 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
     return s
 
 
+_WDFT_CACHE: dict = {}
+
+
+def _spectral_detrend_table(s):
+    """Low-bin window spectrum (device complex64) enabling the constant detrend as a spectral
+    correction in the fused welch kernel, or None (time-domain detrend)."""
+    if s.code != 1 or s.nperseg != s.nfft or 2 * s.nstep != s.nperseg:
+        return None
+    w32 = (s.win_np * np.sqrt(s.scale)).astype(np.float32)
+    key = (w32.tobytes(), s.nfft)
+    hit = _WDFT_CACHE.get(key, False)
+    if hit is False:
+        low = _kernels.window_low_spectrum(w32, s.nfft)
+        hit = None if low is None else device_vector(low[0], dtype=torch.complex64)
+        if len(_WDFT_CACHE) >= 64:
+            _WDFT_CACHE.clear()
+        _WDFT_CACHE[key] = hit
+    return hit
+
+
 def _materialize_frames_input(s) -> tuple[torch.Tensor, torch.Tensor | None]:
     """Boundary extension and padding applied explicitly (composed path only)."""
     X, Y = s.X, s.Y
@@ -339,7 +359,7 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
         rows = int(np.prod(outer)) if outer else 1
         if same:
             res = _kernels.welch_mean(X.reshape(rows, n), s.win, s.nperseg, s.nfft, s.nstep,
-                                      s.code, s.onesided)
+                                      s.code, s.onesided, wdft=_spectral_detrend_table(s))
         else:
             Xb = X.expand(outer + (n,)).reshape(rows, n)
             Yb = Y.expand(outer + (n,)).reshape(rows, n)

@@ -226,3 +226,37 @@ def test_torch_inputs_and_outputs(rng):
     torch.testing.assert_close(p1, p2, rtol=0, atol=0)
     f3, p3 = msig.welch(torch.from_numpy(x), nperseg=512)
     torch.testing.assert_close(p1, p3, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("window", ["hann", "hamming", "blackman", "boxcar", ("tukey", 0.25)])
+@pytest.mark.parametrize("offset", [0.0, 0.5, 4.0])
+def test_half_overlap_detrend_paths(rng, window, offset):
+    """50%-overlap fused welch: the spectral constant detrend (sparse window spectra) and the
+    time-domain one (tukey) against scipy, including signals with a DC offset."""
+    from mlx_signal_b200 import _kernels
+
+    nper = 1024
+    x = (rng.standard_normal((4, 40 * nper)) + offset).astype(np.float32)
+    w = sps.get_window(window, nper)
+    sparse = _kernels.window_low_spectrum((w * 0.01).astype(np.float32), nper) is not None
+    assert sparse == (window != ("tukey", 0.25))
+    _, p = msig.welch(x, window=window, nperseg=nper, fs=48000.0)
+    _, p_ref = sps.welch(x.astype(np.float64), window=window, nperseg=nper, fs=48000.0)
+    assert_close(p, p_ref, rtol=1e-4, atol_frac=1e-5)
+    err = max(rel_err_bins(p[c], p_ref[c]) for c in range(4))
+    assert err <= (1e-5 if offset <= 0.5 else 1e-4), err
+
+
+def test_spectral_and_time_domain_detrend_agree(rng):
+    from mlx_signal_b200 import _kernels
+
+    nper = 256
+    x = torch.from_numpy(rng.standard_normal((8, 300 * nper)).astype(np.float32)).cuda()
+    w = sps.get_window("hann", nper).astype(np.float32)
+    low = _kernels.window_low_spectrum(w, nper)
+    assert low is not None and low[1] == 2
+    wt = torch.from_numpy(w).cuda()
+    a = _kernels.welch_mean(x, wt, nper, nper, nper // 2, 1, True)
+    b = _kernels.welch_mean(x, wt, nper, nper, nper // 2, 1, True,
+                            wdft=torch.from_numpy(low[0]).cuda())
+    torch.testing.assert_close(a, b, rtol=2e-5, atol=1e-6 * float(a.max()))
