@@ -355,6 +355,16 @@ def secondary(x, steps, warmup, dist, clocks):
     nseg_s = (NSAMP + NPERSEG - NPERSEG) // HOP + 1
     b = C * NSAMP * 4 + C * nseg_s * NBINS * 8
     out["stft_64x2p20"] = {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak}
+    # istft of that stft (fused inverse FFT + overlap-add + normalisation), round-trip error
+    z = _kernels.frames("stft", x, wsp, NPERSEG, NPERSEG, HOP, 0, True, ext=NPERSEG // 2,
+                        ext_mode="zeros", n_total=NSAMP + NPERSEG)
+    wsum = float(win.double().sum())
+    ms = timed(lambda: _kernels.istft_fused(z, win, wsum, NPERSEG, HOP), k, warmup, dist, clocks)
+    xr = _kernels.istft_fused(z, win, wsum, NPERSEG, HOP)[:, NPERSEG // 2 : NPERSEG // 2 + NSAMP]
+    rt = float((xr - x).abs().max() / x.abs().max())
+    b = C * nseg_s * NBINS * 8 + C * NSAMP * 4
+    out["istft_64x2p20"] = {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
+                            "roundtrip_max_err_rel_peak": rt}
     return out
 
 

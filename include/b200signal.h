@@ -158,6 +158,20 @@ SP_API int sp_csd_frames_c64(const float* x, const float* y, int64_t rows, int64
                              int64_t ldx, int64_t ldy, const float* win, int nperseg, int nfft,
                              int hop, int detrend, int onesided, float* out, void* stream);
 
+/*
+ * Fused inverse STFT of one-sided spectra: z is (rows, nseg, ldf) complex64 (row stride ld_row
+ * complex elements), bins k < nbins_in used, missing bins up to nperseg/2 taken as zero, the
+ * DC and Nyquist bins taken as real (irfft semantics). Output: (rows, outlen) float32 with
+ * outlen = nperseg + (nseg-1)*hop, x = OLA(irfft(z) * win * scale) / norm where
+ * norm = OLA(win^2) and samples with norm <= 1e-10 are not divided (scipy's rule); the caller
+ * trims the boundary. nperseg (== nfft) must be a power of two in [2, 4096].
+ * Replaces _stft_metal.istft_frames (_stft_metal.py:851-887: _ISTFT_SRC :753-795 then the
+ * gather OLA _OLA_SRC :797-820) and the norm division of spectral.istft (spectral.py:929-943).
+ */
+SP_API int sp_istft_f32(const float* z, int64_t rows, int nseg, int64_t ld_row, int ldf,
+                        int nbins_in, const float* win, float scale, int nperseg, int hop,
+                        float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         c_i,
         [c_fp, c_fp, c_i64, c_i64, c_i64, c_i64, c_fp, c_i, c_i, c_i, c_i, c_i, c_fp, c_p],
     ),
+    "sp_istft_f32": (
+        c_i,
+        [c_fp, c_i64, c_i, c_i64, c_i, c_i, c_fp, ctypes.c_float, c_i, c_i, c_fp, c_p],
+    ),
 }
 
 SP_OK = 0

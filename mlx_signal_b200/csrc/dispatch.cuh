@@ -7,6 +7,7 @@
 #include <utility>
 
 #include "frame_kernels.cuh"
+#include "istft_kernels.cuh"
 #include "mean_kernels.cuh"
 
 namespace b2s {
@@ -39,6 +40,8 @@ struct KernelInfo {
 
 using MeanInfo = KernelInfo<MeanParams>;
 using FrameInfo = KernelInfo<FrameParams>;
+using IstftInfo = KernelInfo<IstftParams>;
+IstftInfo istft_lookup(int log_l);  // log_l in [1, kMaxLogL]
 
 // family: 0 welch mean, 1 cross mean
 MeanInfo mean_lookup_welch(int log_l, int det);

@@ -1,0 +1,182 @@
+// Fused inverse STFT: per-frame inverse real FFT, synthesis window, overlap-add and the
+// window-energy normalisation in one pass (power-of-two nperseg == nfft, one-sided input).
+//
+// Reference behaviour replaced: _stft_metal.istft_frames (src/mlx_signal_processing/
+// _stft_metal.py:851-887) -- kernel _ISTFT_SRC (:753-795) writes windowed frames to device
+// memory, then _OLA_SRC (:797-820) re-reads them to gather the overlap-add -- plus the norm
+// division of spectral.istft (spectral.py:929-943, 982). Differences by design:
+//  * two consecutive frames share one complex inverse FFT: with X_s, X_{s+1} extended
+//    Hermitian-symmetrically, IFFT(X_s + i X_{s+1}) = x_s + i x_{s+1} (both real);
+//  * each team owns a contiguous output range and accumulates the overlap-add in a
+//    shared-memory ring buffer, recomputing the few halo frames that reach into its range from
+//    the left, so every output sample is summed in a fixed order by one team (deterministic,
+//    no second pass over HBM);
+//  * the normalisation sum_s win^2[t - s hop] comes from a per-CTA periodic table in the
+//    interior and is summed directly near the row ends; samples with norm <= 1e-10 are not
+//    divided (scipy's rule).
+#pragma once
+
+#include "fft_core.cuh"
+#include "mean_kernels.cuh"
+#include "team_util.cuh"
+
+namespace b2s {
+
+struct IstftParams {
+  const float2* z;   // (rows, nseg, ldf) complex64 one-sided spectra, bins k < nbins_in valid
+  int64_t ld_row;    // complex elements between rows
+  int ldf;           // complex elements between frames
+  int nbins_in;      // valid bins per frame (missing bins up to L/2 are zero)
+  int64_t rows;
+  int nseg;
+  int hop;
+  const float* win;  // L window values
+  float scale;       // istft scale (spectrum: sum(win); psd: sqrt(fs sum(win^2)))
+  int64_t outlen;    // L + (nseg - 1) * hop
+  float* out;        // (rows, outlen)
+  int64_t G;         // output frames owned per team
+  int64_t total;     // rows * nseg
+};
+
+template <int LOG_L, int LOG_E>
+struct IstftCfg {
+  using PL = Plan<LOG_L, LOG_E>;
+  static constexpr int TEAMS = PL::P >= 64 ? 1 : 128 / PL::P;
+  static constexpr int THREADS = TEAMS * PL::P;
+  static constexpr int SCRATCH = PL::P >= 64 ? PL::P / 32 : 1;
+  static constexpr int WIN = (PL::L + 3) & ~3;
+  // ring of >= 2L floats per team: holds [s*hop, (s+1)*hop + L) for any hop <= L
+  static constexpr int RING = 2 * PL::L;
+  static constexpr size_t SMEM = size_t(TEAMS) * SCRATCH * 16 + size_t(WIN) * 4 * 2 +
+                                 size_t(PL::TW) * 8 + size_t(TEAMS) * PL::BUF * 8 +
+                                 size_t(TEAMS) * RING * 4;
+};
+
+template <int LOG_L, int LOG_E>
+__global__ void __launch_bounds__(IstftCfg<LOG_L, LOG_E>::THREADS) k_istft(IstftParams pr) {
+  using CFG = IstftCfg<LOG_L, LOG_E>;
+  using PL = typename CFG::PL;
+  constexpr int L = PL::L, E = PL::E, P = PL::P, RING = CFG::RING;
+  extern __shared__ float4 smem[];
+  float* weff = reinterpret_cast<float*>(smem + CFG::TEAMS * CFG::SCRATCH);  // win*scale/L
+  float* normp = weff + CFG::WIN;  // periodic window-energy table, index o mod hop
+  float2* tw = reinterpret_cast<float2*>(normp + CFG::WIN);
+  float2* sbuf = tw + PL::TW;
+  float* rings = reinterpret_cast<float*>(sbuf + CFG::TEAMS * PL::BUF);
+  const int hop = pr.hop;
+  const float fs = pr.scale / float(L);
+  for (int i = threadIdx.x; i < L; i += blockDim.x) weff[i] = pr.win[i] * fs;
+  for (int r = threadIdx.x; r < hop; r += blockDim.x) {
+    float s = 0.f;
+    for (int n = r; n < L; n += hop) s = fmaf(pr.win[n], pr.win[n], s);
+    normp[r] = s;
+  }
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+  const unsigned mask = team_mask<P>();
+  float2* buf = sbuf + team * PL::BUF;
+  float* ring = rings + team * RING;
+  for (int i = t; i < RING; i += P) ring[i] = 0.f;
+  team_sync<P>(mask);
+  const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
+  int64_t g = tau * pr.G;
+  const int64_t gend = min(g + pr.G, pr.total);
+  const int halo = (L + hop - 1) / hop - 1;  // frames starting left of a range that reach into it
+  while (g < gend) {
+    const int64_t r = g / pr.nseg;
+    const int f0 = int(g - r * pr.nseg);
+    const int64_t lim = int64_t(f0) + (gend - g);
+    const int f1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
+    // owned output samples: [f0*hop, f1*hop), the last range of a row extends to outlen
+    const int64_t own_lo = int64_t(f0) * hop;
+    const int64_t own_hi = f1 == pr.nseg ? pr.outlen : int64_t(f1) * hop;
+    const int sa = f0 - halo > 0 ? f0 - halo : 0;
+    const float2* zr = pr.z + r * pr.ld_row;
+    float* orow = pr.out + r * pr.outlen;
+    int64_t done = int64_t(sa) * hop;  // samples below this are final (and already written)
+    for (int s = sa; s < f1; s += 2) {
+      const bool two = s + 1 < f1;
+      const float2* za = zr + int64_t(s) * pr.ldf;
+      const float2* zb = za + pr.ldf;
+      float2 v[E];
+      // conj of the Hermitian-extended pair spectrum Z = X_s + i X_{s+1}, DC/Nyquist real
+      static_for<0, E>([&](auto ec) {
+        constexpr int e = decltype(ec)::value;
+        const int k = slot_elem<PL, e>(t);
+        const bool upper = k > L / 2;
+        const int kk = upper ? L - k : k;
+        float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+        if (kk < pr.nbins_in) {
+          a = za[kk];
+          if (two) b = zb[kk];
+        }
+        if (kk == 0 || 2 * kk == L) {
+          a.y = 0.f;
+          b.y = 0.f;
+        }
+        if (upper) {
+          a.y = -a.y;
+          b.y = -b.y;
+        }
+        // Z = a + i b ; conj(Z) = (a.x - b.y, -(a.y + b.x))
+        v[e] = make_float2(a.x - b.y, -(a.y + b.x));
+      });
+      team_pass0<PL>(v);
+      team_passes<PL>(v, buf, tw, t, mask);
+      // x_s[n] = Re(v)/L, x_{s+1}[n] = -Im(v)/L (1/L folded into weff); overlap-add in two
+      // phases so no ring slot is written by two lanes at once
+      const int64_t pa = int64_t(s) * hop;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int n = t + e * P;
+        ring[(pa + n) & (RING - 1)] += v[e].x * weff[n];
+      }
+      team_sync<P>(mask);
+      if (two) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int n = t + e * P;
+          ring[(pa + hop + n) & (RING - 1)] -= v[e].y * weff[n];
+        }
+      }
+      team_sync<P>(mask);
+      // final samples: below the start of the next unprocessed frame (or everything at the end)
+      const bool last = s + 2 >= f1;
+      const int64_t fin = last ? own_hi : int64_t(s + 2) * hop;
+      int res = int((done + t) % hop);  // (o mod hop), advanced incrementally
+      const int pstep = P % hop;
+      for (int64_t o = done + t; o < fin; o += P) {
+        const int slot = int(o & (RING - 1));
+        if (o >= own_lo) {
+          float nrm;
+          if (o >= L - hop && o < int64_t(pr.nseg) * hop) {
+            nrm = normp[res];
+          } else {
+            nrm = 0.f;
+            int64_t slo = o - L + 1 > 0 ? (o - L + 1 + hop - 1) / hop : 0;
+            int64_t shi = o / hop;
+            if (shi > pr.nseg - 1) shi = pr.nseg - 1;
+            for (int64_t q = slo; q <= shi; ++q) {
+              const float w = pr.win[o - q * hop];
+              nrm = fmaf(w, w, nrm);
+            }
+          }
+          const float val = ring[slot];
+          orow[o] = val / (nrm > 1e-10f ? nrm : 1.0f);
+        }
+        ring[slot] = 0.f;
+        res += pstep;
+        if (res >= hop) res -= hop;
+      }
+      done = fin;
+      team_sync<P>(mask);
+    }
+    // partial sums past own_hi belong to the next team's range: clear the ring for the next range
+    for (int i = t; i < RING; i += P) ring[i] = 0.f;
+    team_sync<P>(mask);
+    g += f1 - f0;
+  }
+}
+
+}  // namespace b2s

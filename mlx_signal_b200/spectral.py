@@ -585,9 +585,14 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     time_axis = int(time_axis)
     shape = input_shape(Zxx)
     freq_ax, time_ax, perm = _istft_axes(shape, freq_axis, time_axis)
-    Z = to_device(Zxx)
-    if perm != list(range(Z.dim())):
-        Z = Z.permute(perm)
+    if isinstance(Zxx, np.ndarray):
+        # scipy's stft output is a (freq, time) view of frame-major memory: transposing to
+        # (..., time, freq) first makes the host->device copy contiguous without a host copy
+        Z = to_device(np.transpose(Zxx, perm))
+    else:
+        Z = to_device(Zxx)
+        if perm != list(range(Z.dim())):
+            Z = Z.permute(perm)
     if not Z.is_complex():
         Z = Z.to(torch.complex64)
     nseg = Z.shape[-2]
@@ -628,6 +633,22 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     else:
         raise ValueError(f"Parameter {scaling=} not in ['spectrum', 'psd']!")
     outputlength = nperseg + (nseg - 1) * nstep
+    batch = Z.shape[:-2]
+    if input_onesided and nfft == nperseg and _kernels.is_pow2(nperseg) and \
+            2 <= nperseg <= _kernels.MAX_FUSED_NFFT:
+        rows = int(np.prod(batch)) if batch else 1
+        win = device_vector(win_np.astype(np.float32))
+        x = _kernels.istft_fused(Z.reshape((rows,) + Z.shape[-2:]), win, scale, nperseg, nstep)
+        x = x.reshape(batch + (outputlength,))
+        if boundary:
+            x = x[..., nperseg // 2 : -(nperseg // 2)]
+        if not _nola_ok(win_np, nperseg, nstep, nseg, outputlength, bool(boundary)):
+            warnings.warn(
+                "NOLA condition failed, STFT may not be invertible."
+                + (" Possibly due to missing boundary" if not boundary else ""),
+                stacklevel=2,
+            )
+        return _istft_finish(x, fs, freq_ax, time_ax)
     composed_path_notice("istft", "composed inverse path")
     if input_onesided:
         xsubs = torch.fft.irfft(Z, n=nfft, dim=-1)[..., :nperseg]
@@ -666,9 +687,53 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     x = x / torch.where(norm > 1e-10, norm, torch.ones_like(norm))
     if input_onesided and x.is_complex():
         x = x.real
+    return _istft_finish(x, fs, freq_ax, time_ax)
+
+
+def _istft_finish(x, fs, freq_ax, time_ax):
     n_out = x.shape[-1]
     out_time_axis = time_ax - (1 if freq_ax < time_ax else 0)
     if x.dim() > 1 and out_time_axis != x.dim() - 1:
         x = x.movedim(-1, out_time_axis)
     time = torch.arange(n_out, dtype=torch.float32, device=x.device) / float(fs)
     return time, x
+
+
+def _nola_ok(win_np, nperseg, nstep, nseg, outputlength, boundary) -> bool:
+    """NOLA verdict from the geometry alone (window energy overlap-add > 1e-10 everywhere),
+    computed on the host in float64 and cached: no device synchronisation."""
+    key = (win_np.tobytes(), nperseg, nstep, nseg, outputlength, boundary)
+    hit = _NOLA_CACHE.get(key)
+    if hit is not None:
+        return hit
+    w2 = np.asarray(win_np, dtype=np.float64) ** 2
+    if nseg * nstep >= 4 * nperseg:
+        # interior is periodic in t mod nstep; check the two ends explicitly
+        per = np.zeros(nstep)
+        for j in range(0, nperseg, nstep):
+            seg = w2[j : j + nstep]
+            per[: len(seg)] += seg
+        edge = 2 * nperseg
+        norm = np.zeros(outputlength)
+        for s in range(nseg):
+            lo = s * nstep
+            if lo >= edge and lo + nperseg <= outputlength - edge:
+                continue
+            norm[lo : lo + nperseg] += w2
+        lo_keep = np.concatenate([norm[:edge], norm[outputlength - edge :]])
+        ends = np.concatenate([np.arange(edge), np.arange(outputlength - edge, outputlength)])
+        if boundary:
+            m = (ends >= nperseg // 2) & (ends < outputlength - nperseg // 2)
+            lo_keep = lo_keep[m]
+        ok = bool(np.all(per > 1e-10) and np.all(lo_keep > 1e-10))
+    else:
+        norm = np.zeros(outputlength)
+        for s in range(nseg):
+            norm[s * nstep : s * nstep + nperseg] += w2
+        if boundary:
+            norm = norm[nperseg // 2 : -(nperseg // 2)]
+        ok = bool(np.all(norm > 1e-10))
+    if len(_NOLA_CACHE) >= 256:
+        _NOLA_CACHE.clear()
+    _NOLA_CACHE[key] = ok
+    return ok

@@ -210,3 +210,38 @@ def test_stft_istft_roundtrip_ours(rng):
     t2, x2 = msig.istft(z, nperseg=256)
     x2 = x2.cpu().numpy()[: len(x)]
     np.testing.assert_allclose(x2, x, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize(
+    "nperseg,noverlap,rows,n",
+    [(256, 128, 3, 8000), (1024, 512, 2, 60000), (512, 400, 2, 30000), (128, 27, 4, 7000),
+     (64, 60, 2, 5000), (2048, 1024, 1, 50000), (4096, 3000, 1, 60000), (2, 1, 2, 300)],
+)
+def test_fused_istft_matches_scipy(rng, nperseg, noverlap, rows, n):
+    """Fused inverse FFT + overlap-add + normalisation vs float64 scipy.istft, including hops
+    that do not divide nperseg, team ranges crossing rows and many frames per row."""
+    x = rng.standard_normal((rows, n))
+    _, _, z = sps.stft(x, nperseg=nperseg, noverlap=noverlap)
+    _, x_ref = sps.istft(z, nperseg=nperseg, noverlap=noverlap)
+    _, x_got = msig.istft(z.astype(np.complex64), nperseg=nperseg, noverlap=noverlap)
+    assert tuple(x_got.shape) == x_ref.shape
+    assert_close(x_got, x_ref, rtol=1e-4, atol_frac=1e-5)
+
+
+def test_fused_istft_bin_count_mismatch(rng):
+    """Fewer or more bins than nperseg/2+1 (zero-padded / truncated, as the reference)."""
+    x = rng.standard_normal(6000)
+    _, _, z = sps.stft(x, nperseg=256)
+    for zz in (z[:100], np.concatenate([z, np.ones((7, z.shape[1]))], axis=0)):
+        _, x_ref = sps.istft(zz, nperseg=256, nfft=256, input_onesided=True)
+        _, x_got = msig.istft(zz.astype(np.complex64), nperseg=256, nfft=256)
+        assert_close(x_got, x_ref, rtol=1e-4, atol_frac=1e-5)
+
+
+def test_fused_istft_roundtrip_large(rng):
+    """stft -> istft round trip through the fused kernels on a 16 x 2^18 batch."""
+    x = rng.standard_normal((16, 1 << 18)).astype(np.float32)
+    _, _, z = msig.stft(x, nperseg=1024, noverlap=512)
+    _, x2 = msig.istft(z, nperseg=1024, noverlap=512)
+    err = float((x2[:, : x.shape[1]].cpu() - torch.from_numpy(x)).abs().max())
+    assert err < 1e-5 * float(np.abs(x).max()) * 10, err
