@@ -172,6 +172,39 @@ SP_API int sp_istft_f32(const float* z, int64_t rows, int nseg, int64_t ld_row, 
                         int nbins_in, const float* win, float scale, int nperseg, int hop,
                         float* out, void* stream);
 
+/* Workspace bytes for the long transforms below (two N-point complex intermediates + the device
+ * error word; N = n for sp_fft_c64, n/2 for the real transforms). Negative = error status. */
+SP_API int64_t sp_fft_workspace_size(int64_t n, int batch);
+
+/*
+ * Complex FFT (inverse != 0: inverse FFT including 1/n) of `batch` contiguous rows of n complex64
+ * values, n a power of two in [2^12, 2^26], in three TMA-staged passes; in/out/workspace 16-byte
+ * aligned, out must not alias in. Replaces _fourstep_metal.fft3_last (_fourstep_metal.py:272-303)
+ * and _fourstep._fft_4step_last / _ifft_4step_last (_fourstep.py:100-150).
+ */
+SP_API int sp_fft_c64(const float* in, float* out, int batch, int64_t n, int inverse,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Real-input FFT of `batch` contiguous rows of n float32 (n even, n/2 a power of two in
+ * [2^12, 2^26]): X rows of n/2+1 complex64 bins with row stride ldx_out (complex elements).
+ * Replaces _fourstep.rfft_large (_fourstep.py:213-231) with its untangle (:195-210).
+ */
+SP_API int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t ldx_out,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Inverse real FFT: X rows (stride ldx complex, nbins valid bins, DC/Nyquist taken as real,
+ * missing bins zero) -> batch contiguous rows of n float32 (n even, n/2 a power of two in
+ * [2^12, 2^26]). Replaces _fourstep.irfft_large (_fourstep.py:372-408).
+ */
+SP_API int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, int64_t n,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* Byte offset of the int error word inside a long-transform workspace (0 = ok, SP_ERR_TIMEOUT if
+ * a tile copy wait gave up); read it after synchronising the stream. */
+SP_API int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_t* offset);
+
 #ifdef __cplusplus
 }
 #endif

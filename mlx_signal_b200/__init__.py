@@ -14,6 +14,7 @@ from ._config import (
     get_config,
     set_config,
 )
+from . import fft
 from .spectral import coherence, csd, istft, periodogram, spectrogram, stft, welch
 from .windows import get_window
 
@@ -26,6 +27,7 @@ __all__ = [
     "coherence",
     "config_context",
     "csd",
+    "fft",
     "get_config",
     "get_window",
     "istft",

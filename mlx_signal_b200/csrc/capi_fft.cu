@@ -1,0 +1,268 @@
+// C-ABI: long power-of-two FFTs (three TMA-staged passes) and the packed real transforms.
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "capi_common.h"
+#include "fft3_kernels.cuh"
+
+namespace b2s {
+namespace {
+
+constexpr int kMinLogN = 12, kMaxLogN = 26;
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// digits (R3, R2, R1) of N = 2^e, as balanced as possible (each in [16, 512] for e in [12, 26])
+void digits(int e, int* R3, int* R2, int* R1) {
+  const int a = e / 3, rem = e % 3;
+  *R1 = 1 << (a + (rem > 0 ? 1 : 0));
+  *R2 = 1 << (a + (rem > 1 ? 1 : 0));
+  *R3 = 1 << a;
+}
+
+// 3-D float32 tensor map over rows of 2*d0 floats: dims {2 d0, d1, d2}, box {32, b1, b2},
+// 128B swizzle (the box's 128-byte rows land bank-conflict free for column reads).
+int make_map(CUtensorMap* map, const void* base, int64_t d0, int64_t d1, int64_t d2, int b1,
+             int b2) {
+  auto fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is unavailable from the driver");
+    return SP_ERR_CUDA;
+  }
+  cuuint64_t dims[3] = {cuuint64_t(2 * d0), cuuint64_t(d1), cuuint64_t(d2)};
+  cuuint64_t strides[2] = {cuuint64_t(2 * d0 * 4), cuuint64_t(2 * d0 * d1 * 4)};
+  cuuint32_t box[3] = {32u, cuuint32_t(b1), cuuint32_t(b2)};
+  cuuint32_t estr[3] = {1u, 1u, 1u};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", int(r));
+    return SP_ERR_CUDA;
+  }
+  return SP_OK;
+}
+
+// points per thread of the tile-column FFT of length 2^LOG_L
+template <int LOG_L>
+constexpr int fft3_log_e() {
+  return LOG_L <= 8 ? 4 : 5;
+}
+
+template <int PASS, int LL>
+int launch_one(const CUtensorMap& map, const Fft3Params& p, int blocks, cudaStream_t s) {
+  using CFG = Fft3Cfg<LL, fft3_log_e<LL>()>;
+  auto k = &k_fft3_pass<LL, fft3_log_e<LL>(), PASS>;
+  int dev = 0;
+  B2S_CHECK_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  static std::mutex mu;
+  static bool set_on[64] = {};
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && !set_on[dev]) {
+      B2S_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(CFG::SMEM)),
+                     "fft3 shared-memory attribute");
+      set_on[dev] = true;
+    }
+  }
+  k<<<blocks, CFG::THREADS, CFG::SMEM, s>>>(map, p);
+  B2S_CHECK_CUDA(cudaGetLastError(), "fft3 pass launch");
+  return SP_OK;
+}
+
+template <int PASS>
+int launch_pass(int log_l, const CUtensorMap& map, const Fft3Params& p, int blocks,
+                cudaStream_t s) {
+  switch (log_l) {
+    case 4: return launch_one<PASS, 4>(map, p, blocks, s);
+    case 5: return launch_one<PASS, 5>(map, p, blocks, s);
+    case 6: return launch_one<PASS, 6>(map, p, blocks, s);
+    case 7: return launch_one<PASS, 7>(map, p, blocks, s);
+    case 8: return launch_one<PASS, 8>(map, p, blocks, s);
+    case 9: return launch_one<PASS, 9>(map, p, blocks, s);
+    default:
+      set_error("unsupported pass length 2^%d", log_l);
+      return SP_ERR_UNSUPPORTED;
+  }
+}
+
+// N-point complex FFT of `batch` rows: in -> s1 -> s2 -> out.
+int fft3(const float2* in, float2* s1, float2* s2, float2* out, int batch, int e, int inverse,
+         int* err, cudaStream_t s) {
+  int R3, R2, R1;
+  digits(e, &R3, &R2, &R1);
+  Fft3Params p;
+  p.R1 = R1;
+  p.R2 = R2;
+  p.R3 = R3;
+  p.log_n = e;
+  p.N = int64_t(1) << e;
+  p.batch = batch;
+  p.inverse = inverse;
+  p.err = err;
+  const int l3 = ilog2_exact(R3), l2 = ilog2_exact(R2), l1 = ilog2_exact(R1);
+  CUtensorMap m1, m2, m3;
+  int st;
+  // pass 1 source x[b][m3][m2][r]: dims {2 R1, R2, batch R3}, box {32, 1, min(R3, 256)}
+  if ((st = make_map(&m1, in, R1, R2, int64_t(batch) * R3, 1, R3 < 256 ? R3 : 256))) return st;
+  // pass 2 source S1[b][m2][r][km3]: dims {2 R3, R1, batch R2}, box {32, 1, min(R2, 256)}
+  if ((st = make_map(&m2, s1, R3, R1, int64_t(batch) * R2, 1, R2 < 256 ? R2 : 256))) return st;
+  // pass 3 source S2[b][km2][r][km3]: dims {2 R3, R1, batch R2}, box {32, min(R1, 256), 1}
+  if ((st = make_map(&m3, s2, R3, R1, int64_t(batch) * R2, R1 < 256 ? R1 : 256, 1))) return st;
+  p.in = in;
+  p.out = s1;
+  if ((st = launch_pass<1>(l3, m1, p, batch * R2 * (R1 / kTileCols), s))) return st;
+  p.in = s1;
+  p.out = s2;
+  if ((st = launch_pass<2>(l2, m2, p, batch * R1 * (R3 / kTileCols), s))) return st;
+  p.in = s2;
+  p.out = out;
+  if ((st = launch_pass<3>(l1, m3, p, batch * R2 * (R3 / kTileCols), s))) return st;
+  return SP_OK;
+}
+
+int check_n(int64_t n, int* e) {
+  const int le = ilog2_exact(n);
+  if (le < kMinLogN || le > kMaxLogN) {
+    set_error("long FFT length %lld: needs a power of two in [2^%d, 2^%d]", (long long)n, kMinLogN,
+              kMaxLogN);
+    return SP_ERR_UNSUPPORTED;
+  }
+  *e = le;
+  return SP_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int64_t ws_need(int64_t n_complex, int batch) { return 2 * int64_t(batch) * n_complex * 8 + 256; }
+
+}  // namespace
+}  // namespace b2s
+
+extern "C" {
+
+int64_t sp_fft_workspace_size(int64_t n, int batch) {
+  using namespace b2s;
+  int e;
+  if (batch < 1) {
+    set_error("batch must be >= 1");
+    return SP_ERR_ARG;
+  }
+  const int st = check_n(n, &e);
+  if (st != SP_OK) return st;
+  return ws_need(n, batch);
+}
+
+int sp_fft_c64(const float* in, float* out, int batch, int64_t n, int inverse, void* workspace,
+               size_t workspace_bytes, void* stream) {
+  using namespace b2s;
+  int e;
+  int st = check_n(n, &e);
+  if (st != SP_OK) return st;
+  if (!in || !out || !workspace || batch < 1 || !aligned16(in) || !aligned16(out) ||
+      !aligned16(workspace)) {
+    set_error("sp_fft_c64: null or misaligned (16 B) pointer, or batch < 1");
+    return SP_ERR_ARG;
+  }
+  if (int64_t(workspace_bytes) < ws_need(n, batch)) {
+    set_error("workspace too small: need %lld bytes", (long long)ws_need(n, batch));
+    return SP_ERR_WORKSPACE;
+  }
+  auto s = static_cast<cudaStream_t>(stream);
+  float2* s1 = static_cast<float2*>(workspace);
+  float2* s2 = s1 + int64_t(batch) * n;
+  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * n);
+  B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
+  return fft3(reinterpret_cast<const float2*>(in), s1, s2, reinterpret_cast<float2*>(out), batch,
+              e, inverse, err, s);
+}
+
+int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t ldx_out, void* workspace,
+                size_t workspace_bytes, void* stream) {
+  using namespace b2s;
+  int e;
+  if (n % 2) {
+    set_error("sp_rfft_c64: n must be even");
+    return SP_ERR_UNSUPPORTED;
+  }
+  const int64_t m = n / 2;
+  int st = check_n(m, &e);
+  if (st != SP_OK) return st;
+  if (!x || !X || !workspace || batch < 1 || ldx_out < m + 1 || !aligned16(x) ||
+      !aligned16(workspace) || (reinterpret_cast<uintptr_t>(X) & 7u)) {
+    set_error("sp_rfft_c64: null or misaligned pointer, batch < 1 or ldx_out < n/2+1");
+    return SP_ERR_ARG;
+  }
+  if (int64_t(workspace_bytes) < ws_need(m, batch)) {
+    set_error("workspace too small: need %lld bytes", (long long)ws_need(m, batch));
+    return SP_ERR_WORKSPACE;
+  }
+  auto s = static_cast<cudaStream_t>(stream);
+  float2* s1 = static_cast<float2*>(workspace);
+  float2* s2 = s1 + int64_t(batch) * m;
+  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * m);
+  B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
+  // the n real samples are m interleaved complex values; Z lands in s1 (free after pass 2)
+  if ((st = fft3(reinterpret_cast<const float2*>(x), s1, s2, s1, batch, e, 0, err, s))) return st;
+  const int64_t work = (m / 2 + 1) * batch;
+  k_rfft_untangle<<<unsigned(cdiv(work, 256)), 256, 0, s>>>(s1, reinterpret_cast<float2*>(X), m,
+                                                              batch, ldx_out);
+  B2S_CHECK_CUDA(cudaGetLastError(), "rfft untangle launch");
+  return SP_OK;
+}
+
+int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, int64_t n,
+                 void* workspace, size_t workspace_bytes, void* stream) {
+  using namespace b2s;
+  int e;
+  if (n % 2) {
+    set_error("sp_irfft_f32: n must be even");
+    return SP_ERR_UNSUPPORTED;
+  }
+  const int64_t m = n / 2;
+  int st = check_n(m, &e);
+  if (st != SP_OK) return st;
+  if (!X || !x || !workspace || batch < 1 || nbins < 1 || ldx < nbins || !aligned16(x) ||
+      !aligned16(workspace) || (reinterpret_cast<uintptr_t>(X) & 7u)) {
+    set_error("sp_irfft_f32: null or misaligned pointer or bad sizes");
+    return SP_ERR_ARG;
+  }
+  if (int64_t(workspace_bytes) < ws_need(m, batch)) {
+    set_error("workspace too small: need %lld bytes", (long long)ws_need(m, batch));
+    return SP_ERR_WORKSPACE;
+  }
+  auto s = static_cast<cudaStream_t>(stream);
+  float2* s1 = static_cast<float2*>(workspace);
+  float2* s2 = s1 + int64_t(batch) * m;
+  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * m);
+  B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
+  const int64_t work = (m / 2 + 1) * batch;
+  k_irfft_pretwist<<<unsigned(cdiv(work, 256)), 256, 0, s>>>(
+      reinterpret_cast<const float2*>(X), ldx, nbins, s2, m, batch);
+  B2S_CHECK_CUDA(cudaGetLastError(), "irfft pretwist launch");
+  // Y (in s2) -> S1 (s1) -> S2 (s2, Y already consumed by pass 1) -> x
+  return fft3(s2, s1, s2, reinterpret_cast<float2*>(x), batch, e, 1, err, s);
+}
+
+int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_t* offset) {
+  (void)workspace;
+  if (!offset || batch < 1 || n < 1) return SP_ERR_ARG;
+  *offset = 2 * int64_t(batch) * n * 8;
+  return SP_OK;
+}
+
+}

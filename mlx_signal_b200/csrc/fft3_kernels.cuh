@@ -1,0 +1,295 @@
+// Three-pass (Bailey) power-of-two complex FFT for long transforms, N = R3 * R2 * R1, plus the
+// packed real-input untangle and its inverse.
+//
+// Reference behaviour replaced: _fourstep_metal.fft3_last (src/mlx_signal_processing/
+// _fourstep_metal.py:272-303, kernel sources _P1/_P2/_P3_SRC :90-185) and the large real
+// transforms of _fourstep.py (rfft_large :213-231 with _rfft_untangle :195-210, irfft_large
+// :372-408). Same index maps (the four-step identity applied twice):
+//     n = (m3 R2 + m2) R1 + r,   k = kr (R2 R3) + km2 R3 + km3
+//     x[m3][m2][r] -> S1[m2][r][km3] -> S2[km2][r][km3] -> X[kr][km2][km3]
+//     pass 1: DFT_R3 over m3, twiddle W_N^(R1 m2 km3)      (= W_{R2 R3}^(m2 km3))
+//     pass 2: DFT_R2 over m2, twiddle W_N^(r (km2 R3 + km3))
+//     pass 3: DFT_R1 over r
+// Differences by design:
+//  * every pass stages a 16-column x L-row tile into shared memory with TMA bulk tensor copies
+//    (cp.async.bulk.tensor, 128B swizzle, mbarrier completion, no multicast), so the strided
+//    column walk of the reference's per-thread gather becomes one coalesced bulk transfer;
+//  * each tile column is an L-point team FFT in registers (the spectral kernels' engine);
+//  * inter-pass twiddles are generated per element in FP64 from the exact integer phase
+//    (sincospi of one anchor per lane, then an FP64 recurrence over the lane's E outputs) and
+//    rounded to FP32 once -- no twiddle table in memory;
+//  * the inverse transform is conj(FFT(conj(x))) / N with 1/N folded into pass 1.
+// Every mbarrier wait is bounded; on timeout the CTA records SP_ERR_TIMEOUT in the error word,
+// waits (bounded) for its own copy and returns without touching the data.
+#pragma once
+
+#include <cuda.h>
+
+#include "b200signal.h"
+#include "fft_core.cuh"
+#include "team_util.cuh"
+
+namespace b2s {
+
+struct Fft3Params {
+  const float2* in;    // pass input (pass 1: the signal)
+  float2* out;         // pass output
+  int R1, R2, R3;      // digits, N = R3 * R2 * R1
+  int log_n;
+  int64_t N;
+  int batch;
+  int inverse;         // 1: conj on load (pass 1) and on store (pass 3), scale 1/N in pass 1
+  int* err;            // device error word (0 = ok)
+};
+
+constexpr int kTileCols = 16;                  // columns per tile: 16 complex = 128 B rows
+constexpr uint32_t kMbarSpinLimit = 1u << 22;  // bounded mbarrier polling
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// true when the phase with parity `parity` has completed; bounded polling
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (uint32_t it = 0; it < kMbarSpinLimit; ++it) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 3-D tiled TMA load of one box at coordinates {c0, c1, c2} (no multicast).
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Element (row, col) of a tile whose 128-byte rows were written with the 128B swizzle: the
+// 16-byte chunk index is XORed with (row mod 8).
+__device__ __forceinline__ int swz(int row, int col) {
+  return row * kTileCols + ((((col >> 1) ^ (row & 7)) << 1) | (col & 1));
+}
+
+// FP64 W_N^p = exp(-2 pi i p / N) from the exactly reduced integer phase.
+__device__ __forceinline__ double2 w_exact(int64_t p, int64_t N) {
+  p %= N;
+  double s, c;
+  sincospi(-2.0 * double(p) / double(N), &s, &c);
+  return make_double2(c, s);
+}
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+
+template <int LOG_L, int LOG_E>
+struct Fft3Cfg {
+  using PL = Plan<LOG_L, LOG_E>;
+  static constexpr int L = PL::L;
+  static constexpr int THREADS = kTileCols * PL::P;
+  static constexpr int TILE_BYTES = L * kTileCols * 8;
+  // tile (1024-byte aligned for the swizzle) | exchange buffers | team twiddles | mbarrier
+  static constexpr size_t SMEM = 1024 + size_t(TILE_BYTES) + size_t(kTileCols) * PL::BUF * 8 +
+                                 size_t(PL::TW) * 8 + 16;
+};
+
+// One pass of the three-pass FFT. PASS 1: tile rows m3 (L = R3), columns r; PASS 2: rows m2
+// (L = R2), columns km3; PASS 3: rows r (L = R1), columns km3.
+template <int LOG_L, int LOG_E, int PASS>
+__global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
+    k_fft3_pass(const __grid_constant__ CUtensorMap src, Fft3Params pr) {
+  using CFG = Fft3Cfg<LOG_L, LOG_E>;
+  using PL = typename CFG::PL;
+  constexpr int L = PL::L, E = PL::E, P = PL::P;
+  extern __shared__ unsigned char smraw[];
+  const uintptr_t base = (reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023);
+  float2* tile = reinterpret_cast<float2*>(base);
+  float2* xbuf = tile + L * kTileCols;
+  float2* tw = xbuf + kTileCols * PL::BUF;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + PL::TW);
+  const int R1 = pr.R1, R2 = pr.R2, R3 = pr.R3;
+  const int64_t N = pr.N;
+  // tile coordinates
+  const int colgroups = (PASS == 1 ? R1 : R3) / kTileCols;
+  const int slabs = PASS == 1 ? R2 : (PASS == 2 ? R1 : R2);
+  int bid = blockIdx.x;
+  const int cg = bid % colgroups;
+  bid /= colgroups;
+  const int slab = bid % slabs;
+  const int b = bid / slabs;
+  const int col0 = cg * kTileCols;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(bar, uint32_t(CFG::TILE_BYTES));
+    for (int r0 = 0; r0 < L; r0 += 256) {
+      // box rows run along dim 2 for passes 1/2 ({2 col, slab, b L + row}) and along dim 1
+      // for pass 3 ({2 col, row, b R2 + slab})
+      if constexpr (PASS == 3) {
+        tma_load_3d(tile + r0 * kTileCols, &src, bar, 2 * col0, r0, b * R2 + slab);
+      } else {
+        tma_load_3d(tile + r0 * kTileCols, &src, bar, 2 * col0, slab, b * L + r0);
+      }
+    }
+  }
+  const bool ok = __syncthreads_and(mbar_wait(bar, 0) ? 1 : 0) != 0;
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      atomicExch(pr.err, SP_ERR_TIMEOUT);
+      (void)mbar_wait(bar, 0);  // bounded second wait for the copy still in flight
+    }
+    return;
+  }
+  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+  const unsigned mask = team_mask<P>();
+  float2* buf = xbuf + team * PL::BUF;
+  const int c = team;  // this team's column in the tile
+  float2 v[E];
+  static_for<0, E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    const int row = slot_elem<PL, e>(t);
+    float2 z = tile[swz(row, c)];
+    if (PASS == 1 && pr.inverse) z.y = -z.y;
+    v[e] = z;
+  });
+  team_pass0<PL>(v);
+  team_passes<PL>(v, buf, tw, t, mask);
+  // output k = t + e*P of this column
+  if constexpr (PASS == 1) {
+    // twiddle W_N^(R1 m2 km3), km3 = t + e P; FP64 anchor + recurrence, rounded once
+    const int m2 = slab, r = col0 + c;
+    double2 w = w_exact(int64_t(R1) * m2 * t, N);
+    const double2 d = w_exact(int64_t(R1) * m2 * P, N);
+    const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
+    float2* dst = pr.out + int64_t(b) * N + (int64_t(m2) * R1 + r) * R3;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const float2 wf = make_float2(float(w.x * sc), float(w.y * sc));
+      dst[t + e * P] = cmul(v[e], wf);
+      w = zmul(w, d);
+    }
+  } else {
+    if constexpr (PASS == 2) {
+      // twiddle W_N^(r (km2 R3 + km3)), km2 = t + e P, km3 = col0 + c
+      const int r = slab, km3 = col0 + c;
+      double2 w = w_exact(int64_t(r) * (int64_t(t) * R3 + km3), N);
+      const double2 d = w_exact(int64_t(r) * R3 * P, N);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        v[e] = cmul(v[e], make_float2(float(w.x), float(w.y)));
+        w = zmul(w, d);
+      }
+    }
+    __syncthreads();  // every team has read its column: the tile can be overwritten
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      float2 z = v[e];
+      if (PASS == 3 && pr.inverse) z.y = -z.y;
+      tile[swz(t + e * P, c)] = z;
+    }
+    __syncthreads();
+    // coalesced row stores: row k (L rows) holds 16 consecutive complex outputs
+    //   PASS 2: S2[b][km2 = k][r = slab][km3 = col0 ..], PASS 3: X[b][kr = k][km2 = slab][km3 ..]
+    const int64_t row_stride = PASS == 2 ? int64_t(R1) * R3 : int64_t(R2) * R3;
+    float2* dst = pr.out + int64_t(b) * N + int64_t(slab) * R3 + col0;
+    for (int i = threadIdx.x; i < L * (kTileCols / 2); i += blockDim.x) {
+      const int row = i / (kTileCols / 2), cp = (i % (kTileCols / 2)) * 2;
+      const float2 a0 = tile[swz(row, cp)];
+      const float2 a1 = tile[swz(row, cp + 1)];
+      *reinterpret_cast<float4*>(dst + row * row_stride + cp) = make_float4(a0.x, a0.y, a1.x, a1.y);
+    }
+  }
+}
+
+// Packed real FFT untangle (n = 2m real samples viewed as m complex z, Z = FFT_m(z)):
+//   X_k = (Z_k + conj Z_{m-k})/2 - i w_k (Z_k - conj Z_{m-k})/2, w_k = exp(-i pi k/m), k < m;
+//   X_m = Re Z_0 - Im Z_0. One thread per k in [0, m/2]: it produces X_k and X_{m-k}.
+__global__ void k_rfft_untangle(const float2* __restrict__ Z, float2* __restrict__ X, int64_t m,
+                                int batch, int64_t ldx) {
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t half = m / 2 + 1;
+  if (idx >= half * batch) return;
+  const int64_t b = idx / half, k = idx - b * half;
+  const float2* z = Z + b * m;
+  float2* x = X + b * ldx;
+  if (k == 0) {
+    const float2 z0 = z[0];
+    x[0] = make_float2(z0.x + z0.y, 0.f);
+    x[m] = make_float2(z0.x - z0.y, 0.f);
+    return;
+  }
+  const float2 zk = z[k], zm = z[m - k];
+  double s, c;
+  sincospi(-double(k) / double(m), &s, &c);
+  const float2 w = make_float2(float(c), float(s));
+  // X_{m-k} shares zk, zm: ze' = conj(ze), zo' = -conj(zo), w_{m-k} = -conj(w_k)
+  const float2 ze = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+  const float2 zo = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));
+  const float2 wz = cmul(w, zo);
+  x[k] = make_float2(ze.x + wz.y, ze.y - wz.x);
+  if (2 * k != m) {
+    const float2 wz2 = make_float2(wz.x, -wz.y);  // w' zo' = conj(w zo)
+    x[m - k] = make_float2(ze.x + wz2.y, -ze.y - wz2.x);
+  }
+}
+
+// Inverse of the untangle (irfft pre-twist): from X_0..X_m build the packed spectrum
+//   Y_k = E_k + i conj(w_k) O_k, E = (X_k + conj X_{m-k})/2, O = (X_k - conj X_{m-k})/2,
+// with X_0, X_m taken as real; then z = IFFT_m(Y) interleaves the n real samples.
+__global__ void k_irfft_pretwist(const float2* __restrict__ X, int64_t ldx, int nbins,
+                                 float2* __restrict__ Y, int64_t m, int batch) {
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t half = m / 2 + 1;
+  if (idx >= half * batch) return;
+  const int64_t b = idx / half, k = idx - b * half;
+  const float2* x = X + b * ldx;
+  float2* y = Y + b * m;
+  auto get = [&](int64_t j) -> float2 {
+    if (j >= nbins) return make_float2(0.f, 0.f);
+    float2 v = x[j];
+    if (j == 0 || j == m) v.y = 0.f;
+    return v;
+  };
+  const float2 xk = get(k), xm = get(m - k);
+  double s, c;
+  sincospi(-double(k) / double(m), &s, &c);
+  const float2 wc = make_float2(float(c), float(-s));  // conj(w_k)
+  const float2 e1 = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
+  const float2 o1 = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
+  const float2 t1 = cmul(wc, o1);
+  y[k % m] = make_float2(e1.x - t1.y, e1.y + t1.x);
+  if (k != 0 && 2 * k != m) {
+    // index m-k: E' = conj(E), O' = -conj(O), conj(w_{m-k}) = -w_k
+    const float2 e2 = make_float2(e1.x, -e1.y);
+    const float2 o2 = make_float2(-o1.x, o1.y);
+    const float2 wc2 = make_float2(-float(c), -float(s));
+    const float2 t2 = cmul(wc2, o2);
+    y[m - k] = make_float2(e2.x - t2.y, e2.y + t2.x);
+  }
+}
+
+}  // namespace b2s

@@ -1,0 +1,128 @@
+"""Long power-of-two FFTs on B200: rfft / irfft / fft / ifft along one axis.
+
+Counterpart of the reference's FFT routing for long transforms (src/mlx_signal_processing/
+_fft_core.py:55-104 -> _fourstep.rfft_large / irfft_large / fft_large / ifft_large,
+_fourstep.py:177-231, 372-408 -> _fourstep_metal.fft3_last for 2^21..2^26). Lengths whose
+(half-)length is a power of two in [2^12, 2^26] run the three-pass TMA-staged kernels; other
+lengths run cuFFT through torch.fft (the composed GPU path; the reference uses MLX's own FFT
+there). numpy.fft semantics for `n` (zero-pad or truncate) and `axis`.
+"""
+
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import _lib
+from ._array import stream_handle, to_device
+from ._config import composed_path_notice
+
+__all__ = ["fft", "ifft", "irfft", "rfft"]
+
+MIN_LOG2, MAX_LOG2 = 12, 26
+
+
+def _pow2_in_range(m: int) -> bool:
+    return m >= 1 and (m & (m - 1)) == 0 and MIN_LOG2 <= m.bit_length() - 1 <= MAX_LOG2
+
+
+def _last(t: torch.Tensor, axis: int) -> torch.Tensor:
+    return t.movedim(axis, -1) if t.dim() > 1 and axis not in (-1, t.dim() - 1) else t
+
+
+def _back(t: torch.Tensor, axis: int) -> torch.Tensor:
+    return t.movedim(-1, axis) if t.dim() > 1 and axis not in (-1, t.dim() - 1) else t
+
+
+def _fit(t: torch.Tensor, n: int) -> torch.Tensor:
+    cur = t.shape[-1]
+    if cur == n:
+        return t
+    if cur > n:
+        return t[..., :n]
+    pad = torch.zeros(t.shape[:-1] + (n - cur,), dtype=t.dtype, device=t.device)
+    return torch.cat([t, pad], dim=-1)
+
+
+def _workspace(n_complex: int, batch: int, dev) -> torch.Tensor:
+    nbytes = _lib.load().sp_fft_workspace_size(n_complex, batch)
+    if nbytes < 0:
+        _lib.check(int(nbytes), "sp_fft_workspace_size")
+    return torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+
+
+def rfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
+    """One-sided FFT of real input (complex64 out, n//2+1 bins)."""
+    x = to_device(a)
+    if x.is_complex():
+        x = x.real
+    x = _last(x, axis)
+    n = x.shape[-1] if n is None else int(n)
+    x = _fit(x, n)
+    if n % 2 == 0 and _pow2_in_range(n // 2):
+        batch = tuple(x.shape[:-1])
+        rows = math.prod(batch)
+        xr = x.reshape(rows, n).contiguous()
+        out = torch.empty((rows, n // 2 + 1), dtype=torch.complex64, device=x.device)
+        ws = _workspace(n // 2, rows, x.device)
+        _lib.check(_lib.load().sp_rfft_c64(xr.data_ptr(), out.data_ptr(), rows, n, n // 2 + 1,
+                                           ws.data_ptr(), ws.numel(), stream_handle()),
+                   "sp_rfft_c64")
+        return _back(out.reshape(batch + (n // 2 + 1,)), axis)
+    composed_path_notice("rfft", "length outside the three-pass kernels")
+    return _back(torch.fft.rfft(x, n=n, dim=-1), axis)
+
+
+def irfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
+    """Inverse of rfft: real float32 output of length n (default 2*(bins-1))."""
+    X = to_device(a)
+    if not X.is_complex():
+        X = X.to(torch.complex64)
+    X = _last(X, axis)
+    n = 2 * (X.shape[-1] - 1) if n is None else int(n)
+    if n % 2 == 0 and _pow2_in_range(n // 2):
+        batch = tuple(X.shape[:-1])
+        rows = math.prod(batch)
+        nb = min(X.shape[-1], n // 2 + 1)
+        Xr = X[..., :nb].reshape(rows, nb).contiguous()
+        out = torch.empty((rows, n), dtype=torch.float32, device=X.device)
+        ws = _workspace(n // 2, rows, X.device)
+        _lib.check(_lib.load().sp_irfft_f32(Xr.data_ptr(), nb, nb, out.data_ptr(), rows, n,
+                                            ws.data_ptr(), ws.numel(), stream_handle()),
+                   "sp_irfft_f32")
+        return _back(out.reshape(batch + (n,)), axis)
+    composed_path_notice("irfft", "length outside the three-pass kernels")
+    return _back(torch.fft.irfft(X, n=n, dim=-1), axis)
+
+
+def _cfft(a, n, axis, inverse: bool) -> torch.Tensor:
+    z = to_device(a)
+    if not z.is_complex():
+        z = z.to(torch.complex64)
+    z = _last(z, axis)
+    n = z.shape[-1] if n is None else int(n)
+    z = _fit(z, n)
+    if _pow2_in_range(n):
+        batch = tuple(z.shape[:-1])
+        rows = math.prod(batch)
+        zr = z.reshape(rows, n).contiguous()
+        out = torch.empty((rows, n), dtype=torch.complex64, device=z.device)
+        ws = _workspace(n, rows, z.device)
+        _lib.check(_lib.load().sp_fft_c64(zr.data_ptr(), out.data_ptr(), rows, n, int(inverse),
+                                          ws.data_ptr(), ws.numel(), stream_handle()),
+                   "sp_fft_c64")
+        return _back(out.reshape(batch + (n,)), axis)
+    composed_path_notice("fft", "length outside the three-pass kernels")
+    f = torch.fft.ifft if inverse else torch.fft.fft
+    return _back(f(z, n=n, dim=-1), axis)
+
+
+def fft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
+    """Complex FFT along `axis` (complex64 out)."""
+    return _cfft(a, n, axis, False)
+
+
+def ifft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
+    """Inverse complex FFT along `axis`, including 1/n."""
+    return _cfft(a, n, axis, True)

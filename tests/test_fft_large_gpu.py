@@ -1,0 +1,103 @@
+"""GPU parity: the three-pass long FFTs against float64 numpy (ports of the reference's
+tests/test_fourstep.py: sizes 2^21..2^23, both directions, batched/axis, padding, structured
+signals, round trip), plus the largest sizes and the error word."""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from mlx_signal_b200 import fft as bfft
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(got, ref):
+    got = got.cpu().numpy() if isinstance(got, torch.Tensor) else got
+    return float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-30))
+
+
+@pytest.mark.parametrize("e", [12, 16, 21, 22, 23])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_fft3_matches_numpy(rng, e, inverse):
+    n = 1 << e
+    x = (rng.standard_normal((2, n)) + 1j * rng.standard_normal((2, n))).astype(np.complex64)
+    got = (bfft.ifft if inverse else bfft.fft)(x)
+    ref = (np.fft.ifft if inverse else np.fft.fft)(x.astype(np.complex128), axis=-1)
+    for i in range(2):
+        assert _rel(got[i], ref[i]) < 2e-6
+
+
+@pytest.mark.parametrize("e", [13, 22, 23, 24])
+def test_rfft_irfft_large(rng, e):
+    n = 1 << e
+    x = rng.standard_normal(n).astype(np.float32)
+    ref = np.fft.rfft(x.astype(np.float64))
+    got = bfft.rfft(x)
+    assert tuple(got.shape) == ref.shape
+    assert _rel(got, ref) < 5e-6
+    back = bfft.irfft(got, n=n)
+    assert _rel(back, x) < 5e-6
+
+
+@pytest.mark.parametrize("e", [25, 26])
+def test_fft3_largest_sizes(rng, e):
+    n = 1 << e
+    x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    assert _rel(bfft.fft(x), np.fft.fft(x.astype(np.complex128))) < 2e-6
+
+
+def test_batched_and_axis(rng):
+    n = 1 << 21
+    x = rng.standard_normal((3, n)).astype(np.float32)
+    ref = np.fft.rfft(x.astype(np.float64), axis=-1)
+    assert _rel(bfft.rfft(x, axis=-1), ref) < 5e-6
+    xt = np.ascontiguousarray(x.T)
+    ref0 = np.fft.rfft(xt.astype(np.float64), axis=0)
+    got0 = bfft.rfft(xt, axis=0)
+    assert tuple(got0.shape) == ref0.shape
+    assert _rel(got0, ref0) < 5e-6
+
+
+def test_padding_semantics(rng):
+    x = rng.standard_normal(1_500_000).astype(np.float32)
+    n = 1 << 21
+    assert _rel(bfft.rfft(x, n=n), np.fft.rfft(x.astype(np.float64), n=n)) < 5e-6
+
+
+def test_structured_signals():
+    n = 1 << 21
+    t = np.arange(n)
+    tone = np.exp(2j * np.pi * (98765 / n) * t).astype(np.complex64)
+    imp = np.zeros(n, np.complex64)
+    imp[4097] = 1.0
+    for x in (tone, imp):
+        assert _rel(bfft.fft(x), np.fft.fft(x.astype(np.complex128))) < 2e-6
+
+
+def test_roundtrip(rng):
+    n = 1 << 21
+    x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    assert _rel(bfft.ifft(bfft.fft(x)), x) < 2e-6
+
+
+def test_non_pow2_lengths_use_composed_path(rng):
+    x = rng.standard_normal(600_000).astype(np.float32)
+    assert _rel(bfft.rfft(x), np.fft.rfft(x.astype(np.float64))) < 5e-6
+
+
+def test_error_word_clear_after_transform(rng):
+    from mlx_signal_b200 import _lib
+
+    n = 1 << 21
+    x = torch.from_numpy((rng.standard_normal(n) + 0j).astype(np.complex64)).cuda()
+    out = torch.empty_like(x)
+    lib = _lib.load()
+    ws = torch.empty(int(lib.sp_fft_workspace_size(n, 1)), dtype=torch.uint8, device="cuda")
+    assert lib.sp_fft_c64(x.data_ptr(), out.data_ptr(), 1, n, 0, ws.data_ptr(), ws.numel(),
+                          torch.cuda.current_stream().cuda_stream) == 0
+    off = ctypes.c_int64(0)
+    assert lib.sp_fft_error_word(ws.data_ptr(), n, 1, ctypes.byref(off)) == 0
+    torch.cuda.synchronize()
+    assert int(ws[off.value : off.value + 4].view(torch.int32).item()) == 0
