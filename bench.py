@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--serving-seconds", type=float, default=1.0,
+                    help="arrival window per rate of the serving sweep (the config's is 10 s)")
     return ap.parse_args()
 
 
@@ -314,6 +316,56 @@ def timed(fn, steps, warmup, dist=None, clocks=None):
     return ms
 
 
+def serving_sweep(seconds, rates=(1000, 5000, 10000, 20000, 50000), seed=21):
+    """Open-loop Poisson arrivals (70% streaming-STFT chunks of 4096-65536 samples over 256
+    streams, nperseg 1024 / hop 256; 30% welch requests of 1-16 channels x 2^14-2^20 samples,
+    nperseg 256 or 1024) through the continuous-batching server and, on the same schedule,
+    through the plain per-request path. Inputs are resident device views of a 1 GiB pool."""
+    import torch
+
+    import mlx_signal_b200 as msig
+    from mlx_signal_b200 import serving as sv
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    pool = torch.randn(1 << 28, generator=g, device=dev)
+    out = {"arrival_seconds_per_rate": seconds, "hbm_budget_bytes": 4 << 30}
+    # accuracy spot check: batched server results against the plain per-request path
+    srv = sv.SpectralServer(hbm_budget=4 << 30, max_batch=1024, slots=3, keep_results=True)
+    chk = sv.poisson_schedule(20000.0, 0.01, pool, seed=seed + 1)
+    rids = [srv.submit_welch(x, nperseg=p["nperseg"]) if k == sv.KIND_WELCH
+            else srv.submit_chunk(p["stream"], x) for _, k, x, p in chk]
+    srv.drain()
+    worst = 0.0
+    for rid, (_, k, x, p) in zip(rids, chk):
+        if k == sv.KIND_WELCH:
+            ref = msig.welch(x, nperseg=p["nperseg"])[1]
+            got = srv.result(rid)
+            worst = max(worst, float(((got - ref).abs() / ref.abs().clamp_min(1e-30)).max()))
+    out["max_rel_diff_welch_vs_plain_path"] = worst
+    for rate in rates:
+        srv = sv.SpectralServer(hbm_budget=4 << 30, max_batch=1024, slots=3)
+        sv.run_schedule(srv, sv.poisson_schedule(rate, 0.05, pool, seed=seed + 2))  # warm-up
+        srv.stats = sv.ServerStats()
+        sched = sv.poisson_schedule(float(rate), seconds, pool, seed=seed + rate)
+        b = sv.run_schedule(srv, sched).summary()
+        torch.cuda.synchronize()
+        p = sv.run_per_request(sched).summary()
+        torch.cuda.synchronize()
+        out[f"rate_{rate}"] = {
+            "offered": len(sched),
+            "batched": {k: b[k] for k in ("req_per_s", "p50_ms", "p99_ms", "mean_batch",
+                                          "batches", "peak_inflight_bytes")},
+            "per_request": {k: p[k] for k in ("req_per_s", "p50_ms", "p99_ms")},
+            "throughput_ratio": b["req_per_s"] / p["req_per_s"] if p["req_per_s"] else None,
+        }
+        del srv, sched
+    del pool
+    torch.cuda.empty_cache()
+    return out
+
+
 def secondary(x, steps, warmup, dist, clocks):
     """Cheaper side measurements of the other configs (device-resident inputs)."""
     import torch
@@ -365,7 +417,131 @@ def secondary(x, steps, warmup, dist, clocks):
     b = C * nseg_s * NBINS * 8 + C * NSAMP * 4
     out["istft_64x2p20"] = {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
                             "roundtrip_max_err_rel_peak": rt}
+    del y, z, xr
+    out["batched_512_uneven"] = batched_uneven(dist, clocks, peak)
+    out["rfft_1x2p23"] = large_rfft(dist, clocks, peak)
     return out
+
+
+def batched_uneven(dist, clocks, peak, nreq=512, seed=11):
+    """512 independent welch requests (channels ~ U{1..64}, length 2^U(12, 22), nperseg uniform
+    in {256, 1024, 4096}, noverlap = nperseg/2, N(0,1) float32, generated on the device) in ONE
+    persistent launch, against the plain per-request path (one `welch` call each)."""
+    import torch
+    import scipy.signal as sps
+
+    import mlx_signal_b200 as msig
+    from mlx_signal_b200 import _lib, batch as mb
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rs = np.random.default_rng(seed)
+    shapes = []
+    for _ in range(nreq):
+        ch = int(rs.integers(1, 65))
+        N = int(rs.choice([256, 1024, 4096]))
+        n = max(int(2 ** rs.uniform(12, 22)), N)
+        shapes.append((ch, n, N))
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    xs = [torch.randn((ch, n), generator=g, device=dev) for ch, n, _ in shapes]
+    in_bytes = sum(ch * n * 4 for ch, n, _ in shapes)
+    out_bytes = sum(ch * (N // 2 + 1) * 4 for ch, _, N in shapes)
+    jobs = [mb.prepare_welch(x, nperseg=N) for x, (_, _, N) in zip(xs, shapes)]
+    reqs = [j.req for j in jobs]
+    lib = _lib.load()
+    d, w = mb.plan(reqs)
+    addr, count, _owner = mb._as_array(reqs)
+    ws = torch.zeros(w, dtype=torch.uint8, device=dev)
+    host = torch.empty(d, dtype=torch.uint8, pin_memory=True)
+    _lib.check(lib.sp_batch_encode(addr, count, ws.data_ptr(), ws.numel(), host.data_ptr(),
+                                   host.numel()), "sp_batch_encode")
+    desc = host.to(dev)
+
+    def run_batch():
+        _lib.check(lib.sp_batch_run(desc.data_ptr(), ws.data_ptr(), 0,
+                                    torch.cuda.current_stream().cuda_stream), "sp_batch_run")
+
+    ms_b = timed(run_batch, 5, 2, dist, clocks)
+    plain = {}
+
+    def run_plain():
+        for i, (x, (_, _, N)) in enumerate(zip(xs, shapes)):
+            plain[i] = msig.welch(x, nperseg=N)[1]
+
+    ms_p = timed(run_plain, 3, 1, dist, clocks)
+    # accuracy. Per request: max relative error on bins above 1e-6 of each row's peak (requests
+    # averaging >= 8 segments; with fewer, single low-power bins carry float32 FFT rounding
+    # beyond 1e-5) and, for every request, max |error| / max |reference|.
+    def errs(got, ref, nseg):
+        g = got.double()
+        r = ref.double()
+        keep = r.abs() > 1e-6 * r.abs().amax(dim=-1, keepdim=True)
+        rel = float(((g - r).abs()[keep] / r.abs()[keep]).max()) if nseg >= 8 else 0.0
+        return rel, float((g - r).abs().max() / r.abs().max())
+
+    nseg_of = [(n - N) // (N // 2) + 1 for _, n, N in shapes]
+    rel_single = norm_single = 0.0
+    for i, j in enumerate(jobs):
+        a, b2 = errs(j.out, plain[i], nseg_of[i])
+        rel_single, norm_single = max(rel_single, a), max(norm_single, b2)
+    rel_scipy = norm_scipy = 0.0
+    idx = sorted(range(nreq), key=lambda k: shapes[k][0] * shapes[k][1])
+    pick = idx[:4] + [k for k in idx if nseg_of[k] >= 8][:4]
+    for i in pick:
+        _, pref = sps.welch(xs[i].double().cpu().numpy(), nperseg=shapes[i][2])
+        a, b2 = errs(jobs[i].out.cpu(), torch.from_numpy(pref), nseg_of[i])
+        rel_scipy, norm_scipy = max(rel_scipy, a), max(norm_scipy, b2)
+    gbs = (in_bytes + out_bytes) / ms_b / 1e6
+    res = {
+        "requests": nreq,
+        "input_GB": in_bytes / 1e9,
+        "ms_batched": ms_b,
+        "GB/s": gbs,
+        "frac_hbm": gbs / peak,
+        "req_per_s_batched": nreq / ms_b * 1e3,
+        "ms_per_request_plain": ms_p,
+        "req_per_s_plain": nreq / ms_p * 1e3,
+        "speedup_vs_plain": ms_p / ms_b,
+        "vs_single_request_path": {"max_rel_err_bins_nseg_ge_8": rel_single,
+                                   "max_abs_err_rel_peak_all": norm_single},
+        "vs_scipy_f64_8_requests": {"max_rel_err_bins_nseg_ge_8": rel_scipy,
+                                    "max_abs_err_rel_peak_all": norm_scipy},
+        "segments_per_request": {"min": int(min(nseg_of)), "median": int(np.median(nseg_of)),
+                                 "max": int(max(nseg_of))},
+        "launches_per_batch": 1,
+        "grid": int(lib.sp_batch_max_grid()),
+    }
+    del xs, jobs, ws, desc, plain
+    torch.cuda.empty_cache()
+    return res
+
+
+def large_rfft(dist, clocks, peak, log_n=23, seed=5):
+    """1 x 2^23 float32 N(0,1) real FFT through the three-pass path, against numpy float64."""
+    import torch
+
+    from mlx_signal_b200 import _lib
+
+    n = 1 << log_n
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    x = torch.randn(n, generator=g, device=dev)
+    X = torch.empty(n // 2 + 1, dtype=torch.complex64, device=dev)
+    lib = _lib.load()
+    ws = torch.empty(int(lib.sp_fft_workspace_size(n // 2, 1)), dtype=torch.uint8, device=dev)
+
+    def step():
+        _lib.check(lib.sp_rfft_c64(x.data_ptr(), X.data_ptr(), 1, n, n // 2 + 1, ws.data_ptr(),
+                                   ws.numel(), torch.cuda.current_stream().cuda_stream),
+                   "sp_rfft_c64")
+
+    ms = timed(step, 20, 3, dist, clocks)
+    ref = np.fft.rfft(x.double().cpu().numpy())
+    err = float(np.max(np.abs(X.cpu().numpy() - ref)) / np.max(np.abs(ref)))
+    b = n * 4 + (n // 2 + 1) * 8
+    return {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
+            "max_abs_err_rel_peak_vs_numpy_f64": err, "launches": 4}
 
 
 def run_ours(args, rank, world, local_rank, dist):
@@ -424,6 +600,8 @@ def run_ours(args, rank, world, local_rank, dist):
     sec = None
     if not args.no_secondary:
         sec = secondary(x, args.steps, 2, dist, clocks)
+        if args.serving_seconds > 0:
+            sec["serving_poisson"] = serving_sweep(args.serving_seconds)
     clk = clocks.summary()
 
     cpu = None

@@ -205,6 +205,69 @@ SP_API int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int ba
  * a tile copy wait gave up); read it after synchronising the stream. */
 SP_API int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_t* offset);
 
+/* ------------------------------------------------------------------------------------------
+ * Batched persistent launch: many welch requests and streaming-STFT chunks of uneven size and
+ * nperseg in one kernel launch over a device work queue. The reference has no batched form; a
+ * batch replaces one welch (spectral.py:492-526 -> _stft_metal.rfft_power_mean :530-557) or
+ * stft (spectral.py:694-738 -> _stft_metal.rfft_frames :192-220) call per request.
+ *
+ * Usage: sp_batch_plan -> sizes; sp_batch_encode writes the descriptor table into host memory
+ * (pinned, so the caller's host-to-device copy can be asynchronous or graph-captured); the
+ * caller copies it to a device buffer of the same size; sp_batch_run launches. The workspace
+ * must be zero-filled before its first run; every run leaves its queue and counters zero again,
+ * and sp_batch_run's arguments do not depend on the batch, so one captured launch replays for
+ * any batch encoded into the same descriptor buffer and workspace. Outputs must not alias
+ * inputs or one another. Batched classes: nperseg == nfft in {256, 512, 1024, 4096}.
+ * ------------------------------------------------------------------------------------------ */
+enum { SP_BATCH_WELCH = 0, SP_BATCH_STFT_STREAM = 1 };
+
+typedef struct sp_batch_request {
+  int kind;          /* SP_BATCH_WELCH or SP_BATCH_STFT_STREAM */
+  int nperseg;       /* == nfft: 256, 512, 1024 or 4096 */
+  int hop;           /* welch: nperseg/2; stream: 1..nperseg */
+  int detrend;       /* welch: SP_DETREND_NONE or SP_DETREND_CONSTANT (spectral form) */
+  int onesided;      /* welch: 1 one-sided (interior bins doubled), 0 two-sided; stream: 1 */
+  int n_low;         /* welch constant detrend: complex values in win_dft_low (1..nperseg/32) */
+  int seg_per_task;  /* schedule: segments (welch) or frames (stream) per team task; 0 default */
+  int tail_len;      /* stream: samples held in tail_in (0 <= tail_len < nperseg) */
+  int64_t rows;      /* channels / independent rows */
+  int64_t n;         /* samples per row (stream: new samples in this chunk) */
+  int64_t ld;        /* row stride of x, elements */
+  int64_t tail_ld;   /* stream: row stride of tail_in and tail_out (>= nperseg) */
+  const float* x;
+  const float* win;          /* nperseg window values (no scale folded in) */
+  const float* win_dft_low;  /* welch constant detrend: DFT_nperseg(win)[0..n_low) as (re, im) */
+  const float* tail_in;      /* stream: previous tail, rows x tail_ld */
+  float* tail_out;           /* stream: receives the new tail (must differ from tail_in) */
+  float* out;  /* welch: rows x nbins float32 (nbins = nperseg/2+1 or nperseg);
+                  stream: rows x frames x (nperseg/2+1) complex64 */
+  float scale; /* welch: PSD scale (1/(fs*sum w^2) density, 1/(sum w)^2 spectrum);
+                  stream: frame scale (1/sum w for scipy's 'spectrum' stft) */
+} sp_batch_request;
+
+/* Frames a stream chunk of n samples yields after a tail of tail_len samples (frames start every
+ * hop samples of tail || chunk), and the length of the tail it leaves. Negative = error. */
+SP_API int64_t sp_batch_stream_frames(int64_t tail_len, int64_t n, int nperseg, int hop,
+                                      int64_t* new_tail_len);
+
+/* 1 if nperseg is a batched class, else 0. */
+SP_API int sp_batch_supported(int nperseg);
+
+/* Validate a batch; *desc_bytes = descriptor table size, *ws_bytes = workspace size. */
+SP_API int sp_batch_plan(const sp_batch_request* reqs, int nreq, int64_t* desc_bytes,
+                         int64_t* ws_bytes);
+
+/* Write the descriptor table for a batch whose launch will use workspace ws (device). */
+SP_API int sp_batch_encode(const sp_batch_request* reqs, int nreq, void* ws, size_t ws_bytes,
+                           void* desc_host, size_t desc_bytes);
+
+/* Resident CTAs of the batch kernel on the current device (the default persistent grid). */
+SP_API int sp_batch_max_grid(void);
+
+/* Launch a batch from its device descriptor table (grid <= 0: resident maximum). The first run on
+ * a device builds a twiddle table and must not be inside a stream capture. */
+SP_API int sp_batch_run(const void* desc_dev, void* ws, int grid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,12 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "sp_rfft_c64": (c_i, [c_fp, c_fp, c_i, c_i64, c_i64, c_p, c_sz, c_p]),
     "sp_irfft_f32": (c_i, [c_fp, c_i64, c_i, c_fp, c_i, c_i64, c_p, c_sz, c_p]),
     "sp_fft_error_word": (c_i, [c_p, c_i64, c_i, ctypes.POINTER(c_i64)]),
+    "sp_batch_stream_frames": (c_i64, [c_i64, c_i64, c_i, c_i, ctypes.POINTER(c_i64)]),
+    "sp_batch_supported": (c_i, [c_i]),
+    "sp_batch_plan": (c_i, [c_p, c_i, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)]),
+    "sp_batch_encode": (c_i, [c_p, c_i, c_p, c_sz, c_p, c_sz]),
+    "sp_batch_max_grid": (c_i, []),
+    "sp_batch_run": (c_i, [c_p, c_p, c_i, c_p]),
 }
 
 SP_OK = 0

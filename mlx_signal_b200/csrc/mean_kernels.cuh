@@ -165,6 +165,19 @@ struct HalfSmem {
                                   size_t(CFG::TEAMS) * PL::BUF * 8;
 };
 
+// Shared-memory tables and team coordinates used by the half-overlap pair loop.
+template <class PL>
+struct HalfCtx {
+  const float* win;    // L window values
+  const float2* wlo;   // DFT(win)_t for t < P (zero beyond n_low)
+  const float2* whi;   // DFT(win)_{L-P+t}
+  const float2* tw;    // inter-pass twiddles
+  float2* buf;         // team exchange buffer
+  float4* scratch;     // team reduction scratch
+  int t;
+  unsigned mask;
+};
+
 // Welch for the 50%-overlap case nperseg == nfft == L, hop == L/2 (the reference's default
 // noverlap = nperseg/2). A pair of segments (s, s+1) spans three half-blocks A | B | C of the row:
 // x_s = A|B, x_{s+1} = B|C, and the next pair's A is this pair's C. Each half-block is loaded once
@@ -175,13 +188,106 @@ struct HalfSmem {
 // DET == kDetrendConstantSpectral subtracts (m_s + i m_{s+1}) DFT(win)_k after the FFT on the
 // low bins k < n_low and k > L - n_low (the only non-zero window-spectrum bins), which keeps the
 // mean reduction off the FFT's critical path.
+//
+// welch_half_range accumulates sum |Z_k|^2 over the pairs of segments [s0, s1) of one row into
+// acc (bin k = t + e*P in acc[e]).
+template <class PL, int DET>
+__device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const float* __restrict__ xr,
+                                                 int s0, int s1, float (&acc)[PL::E]) {
+  constexpr int L = PL::L, E = PL::E, P = PL::P, H = L / 2, EH = E / 2;
+  constexpr int R0 = PL::radix(0), B0 = E / R0;
+  const int t = c.t;
+  const float inv_n = 1.0f / float(L);
+  float A[EH], B[EH], C[EH];
+  bool carry = false;
+  float sum_c = 0.f;  // team total of the carried half-block (this pair's A)
+  for (int s = s0; s < s1; s += 2) {
+    const bool two = s + 1 < s1;
+    const float* base = xr + int64_t(s) * H;
+    if (s + 3 < s1) {  // warm L2 with the next pair's two new half-blocks
+      for (int o = t * 32; o < 2 * H; o += P * 32)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 3 * H + o));
+    }
+    static_for<0, EH>([&](auto gc) {
+      constexpr int gi = decltype(gc)::value;
+      const int n = slot_elem<PL, 2 * gi>(t);
+      if (!carry) A[gi] = __ldg(base + n);
+      B[gi] = __ldg(base + H + n);
+      C[gi] = two ? __ldg(base + 2 * H + n) : 0.f;
+    });
+    float ma = 0.f, mb = 0.f;
+    if constexpr (DET == kDetrendConstant || DET == kDetrendConstantSpectral) {
+      // block totals: A's comes from the previous pair (its C), so only B and C are reduced
+      float sa = sum_c;
+      if (!carry) {
+        float sums[1] = {tree_sum<EH>([&](auto gc) { return A[decltype(gc)::value]; })};
+        team_sum<P, 1>(sums, c.scratch, c.mask);
+        sa = sums[0];
+      }
+      float sums[2] = {tree_sum<EH>([&](auto gc) { return B[decltype(gc)::value]; }),
+                       tree_sum<EH>([&](auto gc) { return C[decltype(gc)::value]; })};
+      team_sum<P, 2>(sums, c.scratch, c.mask);
+      ma = (sa + sums[0]) * inv_n;
+      mb = two ? (sums[0] + sums[1]) * inv_n : 0.f;
+      sum_c = sums[1];
+    }
+    float2 v[E];
+    static_for<0, EH>([&](auto gc) {
+      constexpr int gi = decltype(gc)::value;
+      const int n = slot_elem<PL, 2 * gi>(t);
+      float2 zl = make_float2(A[gi], two ? B[gi] : 0.f);
+      float2 zh = make_float2(B[gi], C[gi]);
+      if constexpr (DET == kDetrendConstant) {
+        zl = make_float2(zl.x - ma, two ? zl.y - mb : 0.f);
+        zh = make_float2(zh.x - ma, two ? zh.y - mb : 0.f);
+      }
+      const float wl = c.win[n];
+      const float wh = c.win[n + H];
+      const float2 a = make_float2(zl.x * wl, zl.y * wl);
+      v[2 * gi] = make_float2(fmaf(zh.x, wh, a.x), fmaf(zh.y, wh, a.y));
+      v[2 * gi + 1] = make_float2(fmaf(-zh.x, wh, a.x), fmaf(-zh.y, wh, a.y));
+    });
+    static_for<0, B0>([&](auto bc) {
+      constexpr int b = decltype(bc)::value;
+      dft_dit<R0, b * R0, 2>(v);
+    });
+    team_passes<PL>(v, c.buf, c.tw, t, c.mask);
+    if constexpr (DET == kDetrendConstantSpectral) {
+      const float2 m = make_float2(ma, mb);
+      const float2 cl = cmul(m, c.wlo[t]);
+      const float2 ch = cmul(m, c.whi[t]);
+      v[0] = csub(v[0], cl);
+      v[E - 1] = csub(v[E - 1], ch);
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      acc[e] = fmaf(v[e].x, v[e].x, acc[e]);
+      acc[e] = fmaf(v[e].y, v[e].y, acc[e]);
+    }
+#pragma unroll
+    for (int i = 0; i < EH; ++i) A[i] = C[i];
+    carry = true;
+  }
+}
+
+// Load the low-bin window spectrum for the spectral detrend: lo[i] = DFT(win)_i and
+// hi[i] = DFT(win)_{L-P+i} = conj(DFT(win)_{P-i}) (real window), zero at and beyond n_low.
+template <int P>
+__device__ __forceinline__ void load_window_lowbins(float2* lo, float2* hi, const float2* wdft,
+                                                    int n_low, int tid, int nthreads) {
+  for (int i = tid; i < P; i += nthreads) {
+    lo[i] = (wdft != nullptr && i < n_low) ? wdft[i] : make_float2(0.f, 0.f);
+    const int km = P - i;
+    hi[i] = (wdft != nullptr && km < n_low) ? cconj(wdft[km]) : make_float2(0.f, 0.f);
+  }
+}
+
 template <int LOG_L, int LOG_E, int DET>
 __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
     k_welch_half(MeanParams pr) {
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
-  constexpr int L = PL::L, E = PL::E, P = PL::P, H = L / 2, EH = E / 2;
-  constexpr int R0 = PL::radix(0), B0 = E / R0;
+  constexpr int L = PL::L, E = PL::E, P = PL::P;
   extern __shared__ float4 smem[];
   float* win1 = reinterpret_cast<float*>(smem + CFG::TEAMS * CFG::SCRATCH);
   float2* wlo = reinterpret_cast<float2*>(win1 + L);  // DFT(win)_t, t < P
@@ -189,25 +295,24 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
   float2* tw = whi + P;
   float2* sbuf = tw + PL::TW;
   for (int i = threadIdx.x; i < L; i += blockDim.x) win1[i] = pr.win[i];
-  if constexpr (DET == kDetrendConstantSpectral) {
-    // real window: DFT(win)_{L-k} = conj(DFT(win)_k)
-    for (int i = threadIdx.x; i < P; i += blockDim.x) {
-      wlo[i] = i < pr.n_low ? pr.wdft[i] : make_float2(0.f, 0.f);
-      const int km = P - i;  // whi[i] = DFT_{L-P+i} = conj(DFT_{P-i})
-      whi[i] = km < pr.n_low ? cconj(pr.wdft[km]) : make_float2(0.f, 0.f);
-    }
-  }
+  if constexpr (DET == kDetrendConstantSpectral)
+    load_window_lowbins<P>(wlo, whi, pr.wdft, pr.n_low, threadIdx.x, blockDim.x);
   build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
   __syncthreads();
   pdl_trigger();
-  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
-  const unsigned mask = team_mask<P>();
-  float4* scratch = smem + team * CFG::SCRATCH;
-  float2* buf = sbuf + team * PL::BUF;
+  const int team = threadIdx.x / P;
+  HalfCtx<PL> c;
+  c.win = win1;
+  c.wlo = wlo;
+  c.whi = whi;
+  c.tw = tw;
+  c.buf = sbuf + team * PL::BUF;
+  c.scratch = smem + team * CFG::SCRATCH;
+  c.t = threadIdx.x - team * P;
+  c.mask = team_mask<P>();
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
-  const float inv_n = 1.0f / float(L);
   float acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = 0.f;
@@ -216,80 +321,10 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
     const int s0 = int(g - r * pr.nseg);
     const int64_t lim = int64_t(s0) + (gend - g);
     const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
-    const float* xr = pr.x + r * pr.ld_x;
-    float A[EH], B[EH], C[EH];
-    bool carry = false;
-    float sum_c = 0.f;  // team total of the carried half-block (this pair's A)
-    for (int s = s0; s < s1; s += 2) {
-      const bool two = s + 1 < s1;
-      const float* base = xr + int64_t(s) * H;
-      if (s + 3 < s1) {  // warm L2 with the next pair's two new half-blocks
-        for (int o = t * 32; o < 2 * H; o += P * 32)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 3 * H + o));
-      }
-      static_for<0, EH>([&](auto gc) {
-        constexpr int gi = decltype(gc)::value;
-        const int n = slot_elem<PL, 2 * gi>(t);
-        if (!carry) A[gi] = __ldg(base + n);
-        B[gi] = __ldg(base + H + n);
-        C[gi] = two ? __ldg(base + 2 * H + n) : 0.f;
-      });
-      float ma = 0.f, mb = 0.f;
-      if constexpr (DET == kDetrendConstant || DET == kDetrendConstantSpectral) {
-        // block totals: A's comes from the previous pair (its C), so only B and C are reduced
-        float sa = sum_c;
-        if (!carry) {
-          float sums[1] = {tree_sum<EH>([&](auto gc) { return A[decltype(gc)::value]; })};
-          team_sum<P, 1>(sums, scratch, mask);
-          sa = sums[0];
-        }
-        float sums[2] = {tree_sum<EH>([&](auto gc) { return B[decltype(gc)::value]; }),
-                         tree_sum<EH>([&](auto gc) { return C[decltype(gc)::value]; })};
-        team_sum<P, 2>(sums, scratch, mask);
-        ma = (sa + sums[0]) * inv_n;
-        mb = two ? (sums[0] + sums[1]) * inv_n : 0.f;
-        sum_c = sums[1];
-      }
-      float2 v[E];
-      static_for<0, EH>([&](auto gc) {
-        constexpr int gi = decltype(gc)::value;
-        const int n = slot_elem<PL, 2 * gi>(t);
-        float2 zl = make_float2(A[gi], two ? B[gi] : 0.f);
-        float2 zh = make_float2(B[gi], C[gi]);
-        if constexpr (DET == kDetrendConstant) {
-          zl = make_float2(zl.x - ma, two ? zl.y - mb : 0.f);
-          zh = make_float2(zh.x - ma, two ? zh.y - mb : 0.f);
-        }
-        const float wl = win1[n];
-        const float wh = win1[n + H];
-        const float2 a = make_float2(zl.x * wl, zl.y * wl);
-        v[2 * gi] = make_float2(fmaf(zh.x, wh, a.x), fmaf(zh.y, wh, a.y));
-        v[2 * gi + 1] = make_float2(fmaf(-zh.x, wh, a.x), fmaf(-zh.y, wh, a.y));
-      });
-      static_for<0, B0>([&](auto bc) {
-        constexpr int b = decltype(bc)::value;
-        dft_dit<R0, b * R0, 2>(v);
-      });
-      team_passes<PL>(v, buf, tw, t, mask);
-      if constexpr (DET == kDetrendConstantSpectral) {
-        const float2 m = make_float2(ma, mb);
-        const float2 cl = cmul(m, wlo[t]);
-        const float2 ch = cmul(m, whi[t]);
-        v[0] = csub(v[0], cl);
-        v[E - 1] = csub(v[E - 1], ch);
-      }
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        acc[e] = fmaf(v[e].x, v[e].x, acc[e]);
-        acc[e] = fmaf(v[e].y, v[e].y, acc[e]);
-      }
-#pragma unroll
-      for (int i = 0; i < EH; ++i) A[i] = C[i];
-      carry = true;
-    }
+    welch_half_range<PL, DET>(c, pr.x + r * pr.ld_x, s0, s1, acc);
     const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
-    flush_mirror<PL>(acc, pr.partial + (r * pr.cmax + slot) * int64_t(welch_slot_floats(L)), buf,
-                     t, mask);
+    flush_mirror<PL>(acc, pr.partial + (r * pr.cmax + slot) * int64_t(welch_slot_floats(L)),
+                     c.buf, c.t, c.mask);
     g += s1 - s0;
   }
 }
