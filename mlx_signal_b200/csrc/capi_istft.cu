@@ -20,7 +20,8 @@ int sp_istft_f32(const float* z, int64_t rows, int nseg, int64_t ld_row, int ldf
     return SP_ERR_UNSUPPORTED;
   }
   if (rows == 0) return SP_OK;
-  const IstftInfo k = istft_lookup(log_l);
+  const bool half = 2 * hop == nperseg;  // register overlap-add, no ring buffer
+  const IstftInfo k = half ? istft_half_lookup(log_l) : istft_lookup(log_l);
   int sms = 0;
   const int nb = resident_ctas(k.fn, k.threads, k.smem, &sms);
   if (nb <= 0) {
@@ -44,7 +45,13 @@ int sp_istft_f32(const float* z, int64_t rows, int nseg, int64_t ld_row, int ldf
   // at least a few frames per team so the recomputed halo frames stay a small overhead
   const int halo = (nperseg + hop - 1) / hop - 1;
   int64_t G = cdiv(p.total, cap);
-  if (G < 4 * (halo + 1)) G = 4 * (halo + 1);
+  if (half) {
+    // one recomputed frame per team range: keep ranges >= 16 frames, whole pairs
+    if (G < 16) G = 16;
+    G += G & 1;
+  } else if (G < 4 * (halo + 1)) {
+    G = 4 * (halo + 1);
+  }
   p.G = G;
   const int64_t nteams = cdiv(p.total, G);
   const int64_t blocks = cdiv(nteams, k.teams);

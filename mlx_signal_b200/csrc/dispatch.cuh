@@ -41,7 +41,8 @@ struct KernelInfo {
 using MeanInfo = KernelInfo<MeanParams>;
 using FrameInfo = KernelInfo<FrameParams>;
 using IstftInfo = KernelInfo<IstftParams>;
-IstftInfo istft_lookup(int log_l);  // log_l in [1, kMaxLogL]
+IstftInfo istft_lookup(int log_l);       // log_l in [1, kMaxLogL]
+IstftInfo istft_half_lookup(int log_l);  // hop == nperseg / 2
 
 // family: 0 welch mean, 1 cross mean
 MeanInfo mean_lookup_welch(int log_l, int det);

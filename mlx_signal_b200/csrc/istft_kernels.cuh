@@ -179,4 +179,145 @@ __global__ void __launch_bounds__(IstftCfg<LOG_L, LOG_E>::THREADS) k_istft(Istft
   }
 }
 
+// Half-overlap inverse STFT (hop == L/2, scipy's default noverlap): the overlap-add needs no
+// shared-memory ring. With H = L/2 and output block j = [jH, (j+1)H), block j receives the second
+// half of frame j-1 and the first half of frame j. After the pair IFFT of frames (s, s+1) a
+// thread holds sample n = t + e*P of both frames in v[e] (re: frame s, -im: frame s+1), and
+// e < E/2 <=> n < H, so
+//     block s   = carry           + x_s[n]       (n < H)
+//     block s+1 = x_s[n + H]      + x_{s+1}[n]
+//     carry'    = x_{s+1}[n + H]
+// all in registers, stored coalesced. A team owns a contiguous frame range [f0, f1) and writes
+// blocks f0 .. f1-1 (and block nseg, the lone second half of the last frame, when f1 == nseg);
+// it first recomputes frame f0-1 alone for its carry. Interior blocks divide by the periodic
+// window energy w^2[n] + w^2[n+H] (a reciprocal table); blocks 0 and nseg use w^2[n] and
+// w^2[n+H]; samples whose energy is <= 1e-10 are not divided (scipy's rule).
+template <int LOG_L, int LOG_E>
+struct IstftHalfCfg {
+  using PL = Plan<LOG_L, LOG_E>;
+  static constexpr int TEAMS = PL::P >= 64 ? 1 : 128 / PL::P;
+  static constexpr int THREADS = TEAMS * PL::P;
+  static constexpr int H = PL::L / 2 > 0 ? PL::L / 2 : 1;
+  static constexpr size_t SMEM = size_t(PL::L) * 4 + size_t(H) * 4 * 3 + size_t(PL::TW) * 8 +
+                                 size_t(TEAMS) * PL::BUF * 8;
+};
+
+template <class PL>
+__device__ __forceinline__ void istft_load_pair(float2 (&v)[PL::E], const float2* za,
+                                                const float2* zb, bool two, int nbins_in, int t) {
+  constexpr int L = PL::L;
+  // conj of the Hermitian-extended pair spectrum Z = X_s + i X_{s+1}, DC/Nyquist real
+  static_for<0, PL::E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    const int k = slot_elem<PL, e>(t);
+    const bool upper = k > L / 2;
+    const int kk = upper ? L - k : k;
+    float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+    if (kk < nbins_in) {
+      a = __ldg(za + kk);
+      if (two) b = __ldg(zb + kk);
+    }
+    if (kk == 0 || 2 * kk == L) {
+      a.y = 0.f;
+      b.y = 0.f;
+    }
+    if (upper) {
+      a.y = -a.y;
+      b.y = -b.y;
+    }
+    v[e] = make_float2(a.x - b.y, -(a.y + b.x));
+  });
+}
+
+template <int LOG_L, int LOG_E>
+__global__ void __launch_bounds__(IstftHalfCfg<LOG_L, LOG_E>::THREADS)
+    k_istft_half(IstftParams pr) {
+  using CFG = IstftHalfCfg<LOG_L, LOG_E>;
+  using PL = typename CFG::PL;
+  constexpr int L = PL::L, E = PL::E, P = PL::P, H = CFG::H, EH = E / 2;
+  static_assert(E >= 2, "half-overlap istft needs at least two points per thread");
+  extern __shared__ float4 smem[];
+  float* weff = reinterpret_cast<float*>(smem);  // win * scale / L
+  float* inv_mid = weff + L;                     // 1 / (w^2[n] + w^2[n+H]) or 1
+  float* inv_first = inv_mid + H;                // 1 / w^2[n]      (block 0)
+  float* inv_last = inv_first + H;               // 1 / w^2[n + H]  (block nseg)
+  float2* tw = reinterpret_cast<float2*>(inv_last + H);
+  float2* sbuf = tw + PL::TW;
+  const float fs = pr.scale / float(L);
+  for (int i = threadIdx.x; i < L; i += blockDim.x) weff[i] = pr.win[i] * fs;
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    const float a = pr.win[i], b = pr.win[i + H];
+    const float m = fmaf(a, a, b * b), f = a * a, l = b * b;
+    inv_mid[i] = m > 1e-10f ? 1.0f / m : 1.0f;
+    inv_first[i] = f > 1e-10f ? 1.0f / f : 1.0f;
+    inv_last[i] = l > 1e-10f ? 1.0f / l : 1.0f;
+  }
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+  const unsigned mask = team_mask<P>();
+  float2* buf = sbuf + team * PL::BUF;
+  const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
+  int64_t g = tau * pr.G;
+  const int64_t gend = min(g + pr.G, pr.total);
+  while (g < gend) {
+    const int64_t r = g / pr.nseg;
+    const int f0 = int(g - r * pr.nseg);
+    const int64_t lim = int64_t(f0) + (gend - g);
+    const int f1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
+    const float2* zr = pr.z + r * pr.ld_row;
+    float* orow = pr.out + r * pr.outlen;
+    float carry[EH];
+#pragma unroll
+    for (int e = 0; e < EH; ++e) carry[e] = 0.f;
+    if (f0 > 0) {  // second half of frame f0-1
+      float2 v[E];
+      istft_load_pair<PL>(v, zr + int64_t(f0 - 1) * pr.ldf, nullptr, false, pr.nbins_in, t);
+      team_pass0<PL>(v);
+      team_passes<PL>(v, buf, tw, t, mask);
+#pragma unroll
+      for (int e = 0; e < EH; ++e) carry[e] = v[e + EH].x * weff[t + e * P + H];
+      team_sync<P>(mask);
+    }
+    for (int s = f0; s < f1; s += 2) {
+      const bool two = s + 1 < f1;
+      const float2* za = zr + int64_t(s) * pr.ldf;
+      float2 v[E];
+      istft_load_pair<PL>(v, za, za + pr.ldf, two, pr.nbins_in, t);
+      team_pass0<PL>(v);
+      team_passes<PL>(v, buf, tw, t, mask);
+      float* ob = orow + int64_t(s) * H;
+      const float* inv0 = s == 0 ? inv_first : inv_mid;
+#pragma unroll
+      for (int e = 0; e < EH; ++e) {
+        const int n = t + e * P;
+        ob[n] = fmaf(v[e].x, weff[n], carry[e]) * inv0[n];
+      }
+      if (two) {
+        const float* inv1 = inv_mid;  // block s+1 <= nseg-1 is interior
+#pragma unroll
+        for (int e = 0; e < EH; ++e) {
+          const int n = t + e * P;
+          const float val = fmaf(v[e + EH].x, weff[n + H], -v[e].y * weff[n]);
+          ob[H + n] = val * inv1[n];
+          carry[e] = -v[e + EH].y * weff[n + H];
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < EH; ++e) carry[e] = v[e + EH].x * weff[t + e * P + H];
+      }
+      team_sync<P>(mask);
+    }
+    if (f1 == pr.nseg) {  // block nseg: the lone second half of the last frame
+      float* ob = orow + int64_t(pr.nseg) * H;
+#pragma unroll
+      for (int e = 0; e < EH; ++e) {
+        const int n = t + e * P;
+        ob[n] = carry[e] * inv_last[n];
+      }
+    }
+    g += f1 - f0;
+  }
+}
+
 }  // namespace b2s

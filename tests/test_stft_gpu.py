@@ -215,7 +215,8 @@ def test_stft_istft_roundtrip_ours(rng):
 @pytest.mark.parametrize(
     "nperseg,noverlap,rows,n",
     [(256, 128, 3, 8000), (1024, 512, 2, 60000), (512, 400, 2, 30000), (128, 27, 4, 7000),
-     (64, 60, 2, 5000), (2048, 1024, 1, 50000), (4096, 3000, 1, 60000), (2, 1, 2, 300)],
+     (64, 60, 2, 5000), (2048, 1024, 1, 50000), (4096, 3000, 1, 60000), (2, 1, 2, 300),
+     (512, 256, 5, 600), (16, 8, 3, 100), (4096, 2048, 2, 70000)],
 )
 def test_fused_istft_matches_scipy(rng, nperseg, noverlap, rows, n):
     """Fused inverse FFT + overlap-add + normalisation vs float64 scipy.istft, including hops
