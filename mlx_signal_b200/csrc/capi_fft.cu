@@ -1,4 +1,5 @@
 // C-ABI: long power-of-two FFTs (three TMA-staged passes) and the packed real transforms.
+#include <cmath>
 #include <cudaTypedefs.h>
 
 #include <mutex>
@@ -62,31 +63,28 @@ constexpr int fft3_log_e() {
   return LOG_L <= 8 ? 4 : 5;
 }
 
+// Persistent launch: at most the resident CTAs (occupancy x SMs), each walking its share of
+// the pass's `tiles` (resident_ctas also raises the kernel's shared-memory limit per device).
 template <int PASS, int LL>
-int launch_one(const CUtensorMap& map, const Fft3Params& p, int blocks, cudaStream_t s) {
+int launch_one(const CUtensorMap& map, Fft3Params p, int tiles, cudaStream_t s) {
   using CFG = Fft3Cfg<LL, fft3_log_e<LL>()>;
   auto k = &k_fft3_pass<LL, fft3_log_e<LL>(), PASS>;
-  int dev = 0;
-  B2S_CHECK_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
-  static std::mutex mu;
-  static bool set_on[64] = {};
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    if (dev < 64 && !set_on[dev]) {
-      B2S_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          int(CFG::SMEM)),
-                     "fft3 shared-memory attribute");
-      set_on[dev] = true;
-    }
+  int sms = 0;
+  const int nb = resident_ctas(reinterpret_cast<const void*>(k), CFG::THREADS, CFG::SMEM, &sms);
+  if (nb <= 0) {
+    set_error("no resident CTA for the fft3 pass (2^%d points per column)", LL);
+    return SP_ERR_UNSUPPORTED;
   }
-  k<<<blocks, CFG::THREADS, CFG::SMEM, s>>>(map, p);
+  p.ntiles = tiles;
+  const int grid = tiles < nb * sms ? tiles : nb * sms;
+  k<<<grid, CFG::THREADS, CFG::SMEM, s>>>(map, p);
   B2S_CHECK_CUDA(cudaGetLastError(), "fft3 pass launch");
   return SP_OK;
 }
 
 template <int PASS>
 int launch_pass(int log_l, const CUtensorMap& map, const Fft3Params& p, int blocks,
-                cudaStream_t s) {
+                cudaStream_t s) {  // blocks = tiles of the pass
   switch (log_l) {
     case 4: return launch_one<PASS, 4>(map, p, blocks, s);
     case 5: return launch_one<PASS, 5>(map, p, blocks, s);
@@ -114,6 +112,7 @@ int fft3(const float2* in, float2* s1, float2* s2, float2* out, int batch, int e
   p.batch = batch;
   p.inverse = inverse;
   p.err = err;
+  p.ntiles = 0;
   const int l3 = ilog2_exact(R3), l2 = ilog2_exact(R2), l1 = ilog2_exact(R1);
   CUtensorMap m1, m2, m3;
   int st;
@@ -147,6 +146,17 @@ int check_n(int64_t n, int* e) {
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Launch geometry and rotation step of the untangle kernels (kUntT indices per thread).
+unsigned untangle_blocks(int64_t m, int batch) {
+  const int64_t per_row = cdiv(m / 2 + 1, int64_t(kUntB) * kUntT);
+  return unsigned(per_row * batch);
+}
+double2 untangle_step(int64_t m) {
+  // exp(-i pi kUntB / m); kUntB / m is a power of two, so the angle is exact before cos/sin
+  const double a = 3.141592653589793238462643383279502884 * double(kUntB) / double(m);
+  return make_double2(std::cos(a), -std::sin(a));
+}
 
 int64_t ws_need(int64_t n_complex, int batch) { return 2 * int64_t(batch) * n_complex * 8 + 256; }
 
@@ -218,9 +228,8 @@ int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t ldx_out,
   B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
   // the n real samples are m interleaved complex values; Z lands in s1 (free after pass 2)
   if ((st = fft3(reinterpret_cast<const float2*>(x), s1, s2, s1, batch, e, 0, err, s))) return st;
-  const int64_t work = (m / 2 + 1) * batch;
-  k_rfft_untangle<<<unsigned(cdiv(work, 256)), 256, 0, s>>>(s1, reinterpret_cast<float2*>(X), m,
-                                                              batch, ldx_out);
+  k_rfft_untangle<<<untangle_blocks(m, batch), kUntB, 0, s>>>(
+      s1, reinterpret_cast<float2*>(X), m, ldx_out, untangle_step(m));
   B2S_CHECK_CUDA(cudaGetLastError(), "rfft untangle launch");
   return SP_OK;
 }
@@ -250,9 +259,8 @@ int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, in
   float2* s2 = s1 + int64_t(batch) * m;
   int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * m);
   B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
-  const int64_t work = (m / 2 + 1) * batch;
-  k_irfft_pretwist<<<unsigned(cdiv(work, 256)), 256, 0, s>>>(
-      reinterpret_cast<const float2*>(X), ldx, nbins, s2, m, batch);
+  k_irfft_pretwist<<<untangle_blocks(m, batch), kUntB, 0, s>>>(
+      reinterpret_cast<const float2*>(X), ldx, nbins, s2, m, untangle_step(m));
   B2S_CHECK_CUDA(cudaGetLastError(), "irfft pretwist launch");
   // Y (in s2) -> S1 (s1) -> S2 (s2, Y already consumed by pass 1) -> x
   return fft3(s2, s1, s2, reinterpret_cast<float2*>(x), batch, e, 1, err, s);

@@ -40,6 +40,7 @@ struct Fft3Params {
   int batch;
   int inverse;         // 1: conj on load (pass 1) and on store (pass 3), scale 1/N in pass 1
   int* err;            // device error word (0 = ok)
+  int ntiles;          // tiles of this pass (a persistent CTA walks tile, tile + gridDim.x, ...)
 };
 
 constexpr int kTileCols = 16;                  // columns per tile: 16 complex = 128 B rows
@@ -108,13 +109,27 @@ struct Fft3Cfg {
   static constexpr int L = PL::L;
   static constexpr int THREADS = kTileCols * PL::P;
   static constexpr int TILE_BYTES = L * kTileCols * 8;
-  // tile (1024-byte aligned for the swizzle) | exchange buffers | team twiddles | mbarrier
-  static constexpr size_t SMEM = 1024 + size_t(TILE_BYTES) + size_t(kTileCols) * PL::BUF * 8 +
-                                 size_t(PL::TW) * 8 + 16;
+  // two tiles (1024-byte aligned for the swizzle) | exchange buffers | team twiddles | 2 mbarriers
+  static constexpr size_t SMEM = 1024 + 2 * size_t(TILE_BYTES) +
+                                 size_t(kTileCols) * PL::BUF * 8 + size_t(PL::TW) * 8 + 16;
 };
 
 // One pass of the three-pass FFT. PASS 1: tile rows m3 (L = R3), columns r; PASS 2: rows m2
 // (L = R2), columns km3; PASS 3: rows r (L = R1), columns km3.
+// Persistent and double-buffered: a CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...;
+// before waiting for tile i it issues the TMA load of tile i+1 into the other buffer, so the
+// copy overlaps the FFT of tile i. The u-th completion of buffer j's mbarrier is phase u & 1.
+template <int PASS>
+__device__ __forceinline__ void fft3_tile_coords(int tile, int R1, int R2, int R3, int* cg,
+                                                 int* slab, int* b) {
+  const int colgroups = (PASS == 1 ? R1 : R3) / kTileCols;
+  const int slabs = PASS == 1 ? R2 : (PASS == 2 ? R1 : R2);
+  *cg = tile % colgroups;
+  tile /= colgroups;
+  *slab = tile % slabs;
+  *b = tile / slabs;
+}
+
 template <int LOG_L, int LOG_E, int PASS>
 __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
     k_fft3_pass(const __grid_constant__ CUtensorMap src, Fft3Params pr) {
@@ -123,149 +138,177 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
   constexpr int L = PL::L, E = PL::E, P = PL::P;
   extern __shared__ unsigned char smraw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023);
-  float2* tile = reinterpret_cast<float2*>(base);
-  float2* xbuf = tile + L * kTileCols;
+  float2* tiles = reinterpret_cast<float2*>(base);  // two tiles of L x kTileCols
+  float2* xbuf = tiles + 2 * L * kTileCols;
   float2* tw = xbuf + kTileCols * PL::BUF;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + PL::TW);
   const int R1 = pr.R1, R2 = pr.R2, R3 = pr.R3;
   const int64_t N = pr.N;
-  // tile coordinates
-  const int colgroups = (PASS == 1 ? R1 : R3) / kTileCols;
-  const int slabs = PASS == 1 ? R2 : (PASS == 2 ? R1 : R2);
-  int bid = blockIdx.x;
-  const int cg = bid % colgroups;
-  bid /= colgroups;
-  const int slab = bid % slabs;
-  const int b = bid / slabs;
-  const int col0 = cg * kTileCols;
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
   __syncthreads();
-  if (threadIdx.x == 0) {
-    mbar_expect_tx(bar, uint32_t(CFG::TILE_BYTES));
+  auto issue = [&](int tl, int j) {  // thread 0: TMA load of tile tl into buffer j
+    int cg_, slab_, b_;
+    fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg_, &slab_, &b_);
+    float2* dst = tiles + j * (L * kTileCols);
+    mbar_expect_tx(bar + j, uint32_t(CFG::TILE_BYTES));
     for (int r0 = 0; r0 < L; r0 += 256) {
       // box rows run along dim 2 for passes 1/2 ({2 col, slab, b L + row}) and along dim 1
       // for pass 3 ({2 col, row, b R2 + slab})
       if constexpr (PASS == 3) {
-        tma_load_3d(tile + r0 * kTileCols, &src, bar, 2 * col0, r0, b * R2 + slab);
+        tma_load_3d(dst + r0 * kTileCols, &src, bar + j, 2 * cg_ * kTileCols, r0,
+                    b_ * R2 + slab_);
       } else {
-        tma_load_3d(tile + r0 * kTileCols, &src, bar, 2 * col0, slab, b * L + r0);
+        tma_load_3d(dst + r0 * kTileCols, &src, bar + j, 2 * cg_ * kTileCols, slab_,
+                    b_ * L + r0);
       }
     }
-  }
-  const bool ok = __syncthreads_and(mbar_wait(bar, 0) ? 1 : 0) != 0;
-  if (!ok) {
-    if (threadIdx.x == 0) {
-      atomicExch(pr.err, SP_ERR_TIMEOUT);
-      (void)mbar_wait(bar, 0);  // bounded second wait for the copy still in flight
+  };
+  int tl = blockIdx.x;
+  if (threadIdx.x == 0 && tl < pr.ntiles) issue(tl, 0);
+  for (int it = 0; tl < pr.ntiles; ++it, tl += gridDim.x) {
+    const int j = it & 1;
+    const uint32_t par = uint32_t(it >> 1) & 1u;
+    const int nxt = tl + int(gridDim.x);
+    if (threadIdx.x == 0 && nxt < pr.ntiles) issue(nxt, j ^ 1);
+    const bool ok = __syncthreads_and(mbar_wait(bar + j, par) ? 1 : 0) != 0;
+    if (!ok) {
+      if (threadIdx.x == 0) {
+        atomicExch(pr.err, SP_ERR_TIMEOUT);
+        (void)mbar_wait(bar + j, par);  // bounded second waits for the copies still in flight
+        if (nxt < pr.ntiles) (void)mbar_wait(bar + (j ^ 1), uint32_t((it + 1) >> 1) & 1u);
+      }
+      return;
     }
-    return;
-  }
-  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
-  const unsigned mask = team_mask<P>();
-  float2* buf = xbuf + team * PL::BUF;
-  const int c = team;  // this team's column in the tile
-  float2 v[E];
-  static_for<0, E>([&](auto ec) {
-    constexpr int e = decltype(ec)::value;
-    const int row = slot_elem<PL, e>(t);
-    float2 z = tile[swz(row, c)];
-    if (PASS == 1 && pr.inverse) z.y = -z.y;
-    v[e] = z;
-  });
-  team_pass0<PL>(v);
-  team_passes<PL>(v, buf, tw, t, mask);
-  // output k = t + e*P of this column
-  if constexpr (PASS == 1) {
-    // twiddle W_N^(R1 m2 km3), km3 = t + e P; FP64 anchor + recurrence, rounded once
-    const int m2 = slab, r = col0 + c;
-    double2 w = w_exact(int64_t(R1) * m2 * t, N);
-    const double2 d = w_exact(int64_t(R1) * m2 * P, N);
-    const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
-    float2* dst = pr.out + int64_t(b) * N + (int64_t(m2) * R1 + r) * R3;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const float2 wf = make_float2(float(w.x * sc), float(w.y * sc));
-      dst[t + e * P] = cmul(v[e], wf);
-      w = zmul(w, d);
-    }
-  } else {
-    if constexpr (PASS == 2) {
-      // twiddle W_N^(r (km2 R3 + km3)), km2 = t + e P, km3 = col0 + c
-      const int r = slab, km3 = col0 + c;
-      double2 w = w_exact(int64_t(r) * (int64_t(t) * R3 + km3), N);
-      const double2 d = w_exact(int64_t(r) * R3 * P, N);
-#pragma unroll
+    float2* tile = tiles + j * (L * kTileCols);
+    int cg, slab, b;
+    fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg, &slab, &b);
+    const int col0 = cg * kTileCols;
+    const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+    const unsigned mask = team_mask<P>();
+    float2* buf = xbuf + team * PL::BUF;
+    const int c = team;  // this team's column in the tile
+    float2 v[E];
+    static_for<0, E>([&](auto ec) {
+      constexpr int e = decltype(ec)::value;
+      const int row = slot_elem<PL, e>(t);
+      float2 z = tile[swz(row, c)];
+      if (PASS == 1 && pr.inverse) z.y = -z.y;
+      v[e] = z;
+    });
+    team_pass0<PL>(v);
+    team_passes<PL>(v, buf, tw, t, mask);
+    // output k = t + e*P of this column
+    if constexpr (PASS == 1) {
+      // twiddle W_N^(R1 m2 km3), km3 = t + e P; FP64 anchor + recurrence, rounded once
+      const int m2 = slab, r = col0 + c;
+      double2 w = w_exact(int64_t(R1) * m2 * t, N);
+      const double2 d = w_exact(int64_t(R1) * m2 * P, N);
+      const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
+      float2* dst = pr.out + int64_t(b) * N + (int64_t(m2) * R1 + r) * R3;
+  #pragma unroll
       for (int e = 0; e < E; ++e) {
-        v[e] = cmul(v[e], make_float2(float(w.x), float(w.y)));
+        const float2 wf = make_float2(float(w.x * sc), float(w.y * sc));
+        dst[t + e * P] = cmul(v[e], wf);
         w = zmul(w, d);
       }
+    } else {
+      if constexpr (PASS == 2) {
+        // twiddle W_N^(r (km2 R3 + km3)), km2 = t + e P, km3 = col0 + c
+        const int r = slab, km3 = col0 + c;
+        double2 w = w_exact(int64_t(r) * (int64_t(t) * R3 + km3), N);
+        const double2 d = w_exact(int64_t(r) * R3 * P, N);
+  #pragma unroll
+        for (int e = 0; e < E; ++e) {
+          v[e] = cmul(v[e], make_float2(float(w.x), float(w.y)));
+          w = zmul(w, d);
+        }
+      }
+      __syncthreads();  // every team has read its column: the tile can be overwritten
+  #pragma unroll
+      for (int e = 0; e < E; ++e) {
+        float2 z = v[e];
+        if (PASS == 3 && pr.inverse) z.y = -z.y;
+        tile[swz(t + e * P, c)] = z;
+      }
+      __syncthreads();
+      // coalesced row stores: row k (L rows) holds 16 consecutive complex outputs
+      //   PASS 2: S2[b][km2 = k][r = slab][km3 = col0 ..], PASS 3: X[b][kr = k][km2 = slab][km3 ..]
+      const int64_t row_stride = PASS == 2 ? int64_t(R1) * R3 : int64_t(R2) * R3;
+      float2* dst = pr.out + int64_t(b) * N + int64_t(slab) * R3 + col0;
+      for (int i = threadIdx.x; i < L * (kTileCols / 2); i += blockDim.x) {
+        const int row = i / (kTileCols / 2), cp = (i % (kTileCols / 2)) * 2;
+        const float2 a0 = tile[swz(row, cp)];
+        const float2 a1 = tile[swz(row, cp + 1)];
+        *reinterpret_cast<float4*>(dst + row * row_stride + cp) = make_float4(a0.x, a0.y, a1.x, a1.y);
+      }
     }
-    __syncthreads();  // every team has read its column: the tile can be overwritten
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      float2 z = v[e];
-      if (PASS == 3 && pr.inverse) z.y = -z.y;
-      tile[swz(t + e * P, c)] = z;
-    }
-    __syncthreads();
-    // coalesced row stores: row k (L rows) holds 16 consecutive complex outputs
-    //   PASS 2: S2[b][km2 = k][r = slab][km3 = col0 ..], PASS 3: X[b][kr = k][km2 = slab][km3 ..]
-    const int64_t row_stride = PASS == 2 ? int64_t(R1) * R3 : int64_t(R2) * R3;
-    float2* dst = pr.out + int64_t(b) * N + int64_t(slab) * R3 + col0;
-    for (int i = threadIdx.x; i < L * (kTileCols / 2); i += blockDim.x) {
-      const int row = i / (kTileCols / 2), cp = (i % (kTileCols / 2)) * 2;
-      const float2 a0 = tile[swz(row, cp)];
-      const float2 a1 = tile[swz(row, cp + 1)];
-      *reinterpret_cast<float4*>(dst + row * row_stride + cp) = make_float4(a0.x, a0.y, a1.x, a1.y);
-    }
+    __syncthreads();  // buffer j is free for the load of tile it + 2
   }
 }
 
+// Twiddles w_k = exp(-i pi k / m) of the real-FFT untangle and its inverse. A thread handles
+// kUntT indices k = k0 + j * kUntB (j < kUntT): one FP64 sincospi anchor at k0, then an FP64
+// rotation by the launch's step d = exp(-i pi kUntB / m) per index, each rounded to FP32 once.
+constexpr int kUntB = 256;  // threads per block
+constexpr int kUntT = 8;    // indices per thread
+
 // Packed real FFT untangle (n = 2m real samples viewed as m complex z, Z = FFT_m(z)):
 //   X_k = (Z_k + conj Z_{m-k})/2 - i w_k (Z_k - conj Z_{m-k})/2, w_k = exp(-i pi k/m), k < m;
-//   X_m = Re Z_0 - Im Z_0. One thread per k in [0, m/2]: it produces X_k and X_{m-k}.
-__global__ void k_rfft_untangle(const float2* __restrict__ Z, float2* __restrict__ X, int64_t m,
-                                int batch, int64_t ldx) {
-  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+//   X_m = Re Z_0 - Im Z_0. Index k in [0, m/2] produces X_k and X_{m-k}.
+__global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restrict__ Z,
+                                                         float2* __restrict__ X, int64_t m,
+                                                         int64_t ldx, double2 d) {
   const int64_t half = m / 2 + 1;
-  if (idx >= half * batch) return;
-  const int64_t b = idx / half, k = idx - b * half;
+  const int64_t per_row = (half + kUntB * kUntT - 1) / (kUntB * kUntT);
+  const int64_t b = blockIdx.x / per_row;
+  const int64_t k0 = (blockIdx.x - b * per_row) * (kUntB * kUntT) + threadIdx.x;
   const float2* z = Z + b * m;
   float2* x = X + b * ldx;
-  if (k == 0) {
-    const float2 z0 = z[0];
-    x[0] = make_float2(z0.x + z0.y, 0.f);
-    x[m] = make_float2(z0.x - z0.y, 0.f);
-    return;
-  }
-  const float2 zk = z[k], zm = z[m - k];
-  double s, c;
-  sincospi(-double(k) / double(m), &s, &c);
-  const float2 w = make_float2(float(c), float(s));
-  // X_{m-k} shares zk, zm: ze' = conj(ze), zo' = -conj(zo), w_{m-k} = -conj(w_k)
-  const float2 ze = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-  const float2 zo = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));
-  const float2 wz = cmul(w, zo);
-  x[k] = make_float2(ze.x + wz.y, ze.y - wz.x);
-  if (2 * k != m) {
-    const float2 wz2 = make_float2(wz.x, -wz.y);  // w' zo' = conj(w zo)
-    x[m - k] = make_float2(ze.x + wz2.y, -ze.y - wz2.x);
+  double sn, cs;
+  sincospi(-double(k0) / double(m), &sn, &cs);
+  double2 w = make_double2(cs, sn);
+#pragma unroll
+  for (int j = 0; j < kUntT; ++j) {
+    const int64_t k = k0 + int64_t(j) * kUntB;
+    if (k < half) {
+      if (k == 0) {
+        const float2 z0 = z[0];
+        x[0] = make_float2(z0.x + z0.y, 0.f);
+        x[m] = make_float2(z0.x - z0.y, 0.f);
+      } else {
+        const float2 zk = z[k], zm = z[m - k];
+        const float2 wf = make_float2(float(w.x), float(w.y));
+        // X_{m-k} shares zk, zm: ze' = conj(ze), zo' = -conj(zo), w_{m-k} = -conj(w_k)
+        const float2 ze = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 zo = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));
+        const float2 wz = cmul(wf, zo);
+        x[k] = make_float2(ze.x + wz.y, ze.y - wz.x);
+        if (2 * k != m) {
+          const float2 wz2 = make_float2(wz.x, -wz.y);  // w' zo' = conj(w zo)
+          x[m - k] = make_float2(ze.x + wz2.y, -ze.y - wz2.x);
+        }
+      }
+    }
+    w = zmul(w, d);
   }
 }
 
 // Inverse of the untangle (irfft pre-twist): from X_0..X_m build the packed spectrum
 //   Y_k = E_k + i conj(w_k) O_k, E = (X_k + conj X_{m-k})/2, O = (X_k - conj X_{m-k})/2,
 // with X_0, X_m taken as real; then z = IFFT_m(Y) interleaves the n real samples.
-__global__ void k_irfft_pretwist(const float2* __restrict__ X, int64_t ldx, int nbins,
-                                 float2* __restrict__ Y, int64_t m, int batch) {
-  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kUntB) k_irfft_pretwist(const float2* __restrict__ X,
+                                                          int64_t ldx, int nbins,
+                                                          float2* __restrict__ Y, int64_t m,
+                                                          double2 d) {
   const int64_t half = m / 2 + 1;
-  if (idx >= half * batch) return;
-  const int64_t b = idx / half, k = idx - b * half;
+  const int64_t per_row = (half + kUntB * kUntT - 1) / (kUntB * kUntT);
+  const int64_t b = blockIdx.x / per_row;
+  const int64_t k0 = (blockIdx.x - b * per_row) * (kUntB * kUntT) + threadIdx.x;
   const float2* x = X + b * ldx;
   float2* y = Y + b * m;
   auto get = [&](int64_t j) -> float2 {
@@ -274,21 +317,30 @@ __global__ void k_irfft_pretwist(const float2* __restrict__ X, int64_t ldx, int 
     if (j == 0 || j == m) v.y = 0.f;
     return v;
   };
-  const float2 xk = get(k), xm = get(m - k);
-  double s, c;
-  sincospi(-double(k) / double(m), &s, &c);
-  const float2 wc = make_float2(float(c), float(-s));  // conj(w_k)
-  const float2 e1 = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
-  const float2 o1 = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
-  const float2 t1 = cmul(wc, o1);
-  y[k % m] = make_float2(e1.x - t1.y, e1.y + t1.x);
-  if (k != 0 && 2 * k != m) {
-    // index m-k: E' = conj(E), O' = -conj(O), conj(w_{m-k}) = -w_k
-    const float2 e2 = make_float2(e1.x, -e1.y);
-    const float2 o2 = make_float2(-o1.x, o1.y);
-    const float2 wc2 = make_float2(-float(c), -float(s));
-    const float2 t2 = cmul(wc2, o2);
-    y[m - k] = make_float2(e2.x - t2.y, e2.y + t2.x);
+  double sn, cs;
+  sincospi(-double(k0) / double(m), &sn, &cs);
+  double2 w = make_double2(cs, sn);
+#pragma unroll
+  for (int j = 0; j < kUntT; ++j) {
+    const int64_t k = k0 + int64_t(j) * kUntB;
+    if (k < half) {
+      const float2 xk = get(k), xm = get(m - k);
+      const float c = float(w.x), sf = float(w.y);
+      const float2 wc = make_float2(c, -sf);  // conj(w_k)
+      const float2 e1 = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));
+      const float2 o1 = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y + xm.y));
+      const float2 t1 = cmul(wc, o1);
+      y[k % m] = make_float2(e1.x - t1.y, e1.y + t1.x);
+      if (k != 0 && 2 * k != m) {
+        // index m-k: E' = conj(E), O' = -conj(O), conj(w_{m-k}) = -w_k
+        const float2 e2 = make_float2(e1.x, -e1.y);
+        const float2 o2 = make_float2(-o1.x, o1.y);
+        const float2 wc2 = make_float2(-c, -sf);
+        const float2 t2 = cmul(wc2, o2);
+        y[m - k] = make_float2(e2.x - t2.y, e2.y + t2.x);
+      }
+    }
+    w = zmul(w, d);
   }
 }
 
