@@ -78,7 +78,7 @@ struct BatchParams {
 constexpr int kBatchThreads = 128;
 // Shared-memory union over the classes (float4 units): scratch 8 | window 4096 floats | low bins
 // 2 x 128 complex | twiddles 1024 complex (classes <= 1024; 4096 reads a global table) |
-// exchange buffers 4224 complex.
+// exchange buffers 4224 complex (TEAMS x BUF of every class).
 constexpr int kBatchScratchF4 = 8;
 constexpr int kBatchWinFloats = 4096;
 constexpr int kBatchLowBins = 128;
@@ -191,7 +191,8 @@ __device__ __forceinline__ void batch_item(const BatchReqDev* __restrict__ rq, i
       float acc[E];
 #pragma unroll
       for (int e = 0; e < E; ++e) acc[e] = 0.f;
-      welch_half_range<PL, kDetrendConstantSpectral>(c, rq->x + int64_t(row) * ld, s0, s1, acc);
+      welch_half_range<PL, kDetrendConstantSpectral, false, false>(c, rq->x + int64_t(row) * ld,
+                                                                   s0, s1, acc);
       flush_mirror<PL>(acc, rq->part + int64_t(task) * welch_slot_floats(L), c.buf, t, c.mask);
     }
     // Publish this item's partials, then count them against their rows.

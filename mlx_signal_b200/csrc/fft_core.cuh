@@ -181,7 +181,8 @@ struct Plan {
     return s;
   }
   // shared-memory padding: one complex every 2^PADSH keeps the strided Stockham writes and
-  // the contiguous reads bank-conflict free for 8-byte elements.
+  // the contiguous reads bank-conflict free for 8-byte elements. (Two complex per 2^PADSH,
+  // which would allow 128-bit stores of the first exchange, measured slower.)
   static constexpr int PADSH = LOG_E < 4 ? 4 : LOG_E;
   static constexpr int BUF = L + (L >> PADSH);
   __host__ __device__ static constexpr int pad(int a) { return a + (a >> PADSH); }

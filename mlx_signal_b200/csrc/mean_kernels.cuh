@@ -155,20 +155,11 @@ __device__ __forceinline__ void pdl_trigger() {
 }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
-// Shared-memory layout of the half-overlap kernel: scratch | window (L floats) | low-bin window
-// spectrum (2P complex: DFT_L(win)_t and DFT_L(win)_{L-P+t}) | twiddles | exchange buffers.
-template <class CFG>
-struct HalfSmem {
-  using PL = typename CFG::PL;
-  static constexpr size_t BYTES = size_t(CFG::TEAMS) * CFG::SCRATCH * 16 + size_t(PL::L) * 4 +
-                                  size_t(2 * PL::P) * 8 + size_t(PL::TW) * 8 +
-                                  size_t(CFG::TEAMS) * PL::BUF * 8;
-};
-
 // Shared-memory tables and team coordinates used by the half-overlap pair loop.
 template <class PL>
 struct HalfCtx {
-  const float* win;    // L window values
+  const float* win;    // L window values (read when the transposed table is not used)
+  const float4* wt;    // this thread's transposed window row: (w[n_g], w[n_g+H], w[n_g+1], ...)
   const float2* wlo;   // DFT(win)_t for t < P (zero beyond n_low)
   const float2* whi;   // DFT(win)_{L-P+t}
   const float2* tw;    // inter-pass twiddles
@@ -176,6 +167,44 @@ struct HalfCtx {
   float4* scratch;     // team reduction scratch
   int t;
   unsigned mask;
+};
+
+// Transposed window table of the half-overlap kernel: row t (team-local thread) holds, for its
+// register pairs g < E/2, w[n_g] and w[n_g + L/2] with n_g = slot_elem<2g>(t), so a thread reads
+// its whole window with E/4 128-bit loads. Row stride E + 4 floats keeps rows 16-byte aligned and
+// the 8-thread phases of a 128-bit load on disjoint banks.
+template <class PL>
+struct HalfWinT {
+  static constexpr int WS = PL::E + 4;
+  static constexpr int FLOATS = PL::P * WS;
+  static constexpr bool USE = PL::E >= 4;
+};
+
+template <class PL>
+__device__ __forceinline__ void build_half_wint(float* wt, const float* win, int tid) {
+  constexpr int H = PL::L / 2, WS = HalfWinT<PL>::WS;
+  if (tid < PL::P) {
+    float* row = wt + tid * WS;
+    static_for<0, PL::E / 2>([&](auto gc) {
+      constexpr int gi = decltype(gc)::value;
+      const int n = slot_elem<PL, 2 * gi>(tid);
+      row[2 * gi] = win[n];
+      row[2 * gi + 1] = win[n + H];
+    });
+  }
+}
+
+// Shared-memory layout of the half-overlap kernel: scratch | window (transposed table or L floats) |
+// low-bin window
+// spectrum (2P complex: DFT_L(win)_t and DFT_L(win)_{L-P+t}) | twiddles | exchange buffers.
+template <class CFG>
+struct HalfSmem {
+  using PL = typename CFG::PL;
+  // window region: the transposed table (E >= 4) or the plain window, in floats (16-byte multiple)
+  static constexpr int WINF = ((HalfWinT<PL>::USE ? HalfWinT<PL>::FLOATS : PL::L) + 3) & ~3;
+  static constexpr size_t BYTES = size_t(CFG::TEAMS) * CFG::SCRATCH * 16 + size_t(WINF) * 4 +
+                                  size_t(2 * PL::P) * 8 + size_t(PL::TW) * 8 +
+                                  size_t(CFG::TEAMS) * PL::BUF * 8;
 };
 
 // Welch for the 50%-overlap case nperseg == nfft == L, hop == L/2 (the reference's default
@@ -190,19 +219,23 @@ struct HalfCtx {
 // mean reduction off the FFT's critical path.
 //
 // welch_half_range accumulates sum |Z_k|^2 over the pairs of segments [s0, s1) of one row into
-// acc (bin k = t + e*P in acc[e]).
-template <class PL, int DET>
+// acc (bin k = t + e*P in acc[e]). Full pairs run a step without the lone-segment selects; an odd
+// last segment runs the same step with the second segment zero. WT: window from the transposed
+// table (HalfWinT) instead of the plain one. SPLIT = false keeps one loop with a runtime
+// lone-segment flag (less code, for kernels that already run near their register limit).
+template <class PL, int DET, bool WT = false, bool SPLIT = true>
 __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const float* __restrict__ xr,
                                                  int s0, int s1, float (&acc)[PL::E]) {
   constexpr int L = PL::L, E = PL::E, P = PL::P, H = L / 2, EH = E / 2;
   constexpr int R0 = PL::radix(0), B0 = E / R0;
+  static_assert(!WT || HalfWinT<PL>::USE, "transposed window needs E >= 4");
   const int t = c.t;
   const float inv_n = 1.0f / float(L);
   float A[EH], B[EH], C[EH];
   bool carry = false;
   float sum_c = 0.f;  // team total of the carried half-block (this pair's A)
-  for (int s = s0; s < s1; s += 2) {
-    const bool two = s + 1 < s1;
+  auto step = [&](int s, auto two_c) {
+    const bool TWO = bool(two_c);  // a compile-time constant for std::true_type / false_type
     const float* base = xr + int64_t(s) * H;
     if (s + 3 < s1) {  // warm L2 with the next pair's two new half-blocks
       for (int o = t * 32; o < 2 * H; o += P * 32)
@@ -213,7 +246,7 @@ __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const flo
       const int n = slot_elem<PL, 2 * gi>(t);
       if (!carry) A[gi] = __ldg(base + n);
       B[gi] = __ldg(base + H + n);
-      C[gi] = two ? __ldg(base + 2 * H + n) : 0.f;
+      C[gi] = TWO ? __ldg(base + 2 * H + n) : 0.f;
     });
     float ma = 0.f, mb = 0.f;
     if constexpr (DET == kDetrendConstant || DET == kDetrendConstantSpectral) {
@@ -225,28 +258,40 @@ __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const flo
         sa = sums[0];
       }
       float sums[2] = {tree_sum<EH>([&](auto gc) { return B[decltype(gc)::value]; }),
-                       tree_sum<EH>([&](auto gc) { return C[decltype(gc)::value]; })};
+                       TWO ? tree_sum<EH>([&](auto gc) { return C[decltype(gc)::value]; })
+                           : 0.f};
       team_sum<P, 2>(sums, c.scratch, c.mask);
       ma = (sa + sums[0]) * inv_n;
-      mb = two ? (sums[0] + sums[1]) * inv_n : 0.f;
+      mb = TWO ? (sums[0] + sums[1]) * inv_n : 0.f;
       sum_c = sums[1];
     }
     float2 v[E];
-    static_for<0, EH>([&](auto gc) {
+    auto fuse = [&](auto gc, float wl, float wh) {
       constexpr int gi = decltype(gc)::value;
-      const int n = slot_elem<PL, 2 * gi>(t);
-      float2 zl = make_float2(A[gi], two ? B[gi] : 0.f);
+      float2 zl = make_float2(A[gi], TWO ? B[gi] : 0.f);
       float2 zh = make_float2(B[gi], C[gi]);
       if constexpr (DET == kDetrendConstant) {
-        zl = make_float2(zl.x - ma, two ? zl.y - mb : 0.f);
-        zh = make_float2(zh.x - ma, two ? zh.y - mb : 0.f);
+        zl = make_float2(zl.x - ma, TWO ? zl.y - mb : 0.f);
+        zh = make_float2(zh.x - ma, TWO ? zh.y - mb : 0.f);
       }
-      const float wl = c.win[n];
-      const float wh = c.win[n + H];
       const float2 a = make_float2(zl.x * wl, zl.y * wl);
       v[2 * gi] = make_float2(fmaf(zh.x, wh, a.x), fmaf(zh.y, wh, a.y));
       v[2 * gi + 1] = make_float2(fmaf(-zh.x, wh, a.x), fmaf(-zh.y, wh, a.y));
-    });
+    };
+    if constexpr (WT) {
+      static_for<0, EH / 2>([&](auto pc) {
+        constexpr int gp = decltype(pc)::value;
+        const float4 w4 = c.wt[gp];
+        fuse(std::integral_constant<int, 2 * gp>{}, w4.x, w4.y);
+        fuse(std::integral_constant<int, 2 * gp + 1>{}, w4.z, w4.w);
+      });
+    } else {
+      static_for<0, EH>([&](auto gc) {
+        constexpr int gi = decltype(gc)::value;
+        const int n = slot_elem<PL, 2 * gi>(t);
+        fuse(gc, c.win[n], c.win[n + H]);
+      });
+    }
     static_for<0, B0>([&](auto bc) {
       constexpr int b = decltype(bc)::value;
       dft_dit<R0, b * R0, 2>(v);
@@ -267,6 +312,13 @@ __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const flo
 #pragma unroll
     for (int i = 0; i < EH; ++i) A[i] = C[i];
     carry = true;
+  };
+  if constexpr (SPLIT) {
+    int s = s0;
+    for (; s + 1 < s1; s += 2) step(s, std::true_type{});
+    if (s < s1) step(s, std::false_type{});
+  } else {
+    for (int s = s0; s < s1; s += 2) step(s, s + 1 < s1);
   }
 }
 
@@ -288,13 +340,18 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
   constexpr int L = PL::L, E = PL::E, P = PL::P;
+  constexpr bool WT = HalfWinT<PL>::USE;
   extern __shared__ float4 smem[];
   float* win1 = reinterpret_cast<float*>(smem + CFG::TEAMS * CFG::SCRATCH);
-  float2* wlo = reinterpret_cast<float2*>(win1 + L);  // DFT(win)_t, t < P
-  float2* whi = wlo + P;                              // DFT(win)_{L-P+t}
+  float2* wlo = reinterpret_cast<float2*>(win1 + HalfSmem<CFG>::WINF);  // DFT(win)_t, t < P
+  float2* whi = wlo + P;                                              // DFT(win)_{L-P+t}
   float2* tw = whi + P;
   float2* sbuf = tw + PL::TW;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) win1[i] = pr.win[i];
+  if constexpr (WT) {
+    build_half_wint<PL>(win1, pr.win, threadIdx.x);
+  } else {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) win1[i] = pr.win[i];
+  }
   if constexpr (DET == kDetrendConstantSpectral)
     load_window_lowbins<P>(wlo, whi, pr.wdft, pr.n_low, threadIdx.x, blockDim.x);
   build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
@@ -303,6 +360,8 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
   const int team = threadIdx.x / P;
   HalfCtx<PL> c;
   c.win = win1;
+  c.wt = reinterpret_cast<const float4*>(win1) +
+         (threadIdx.x - team * P) * (HalfWinT<PL>::WS / 4);
   c.wlo = wlo;
   c.whi = whi;
   c.tw = tw;
@@ -321,7 +380,7 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
     const int s0 = int(g - r * pr.nseg);
     const int64_t lim = int64_t(s0) + (gend - g);
     const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
-    welch_half_range<PL, DET>(c, pr.x + r * pr.ld_x, s0, s1, acc);
+    welch_half_range<PL, DET, WT>(c, pr.x + r * pr.ld_x, s0, s1, acc);
     const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
     flush_mirror<PL>(acc, pr.partial + (r * pr.cmax + slot) * int64_t(welch_slot_floats(L)),
                      c.buf, c.t, c.mask);
