@@ -89,6 +89,19 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS) k_frames(Frame
       const bool two = KIND != kFrameCross && s + 1 < s1;
       float2 v[E];
       const int64_t sa = int64_t(s) * pr.hop;
+      {  // warm L2 with the samples the next step adds (frames s+2, s+3 / s+1), inside the row
+        constexpr int STEP = KIND == kFrameCross ? 1 : 2;
+        // this step covers [sa, sa + (STEP-1) hop + nperseg); the next adds STEP hops beyond it
+        const int64_t lo = int64_t(sa) - pr.ext + int64_t(STEP - 1) * pr.hop + pr.nperseg;
+        const int64_t hi = lo + int64_t(STEP) * pr.hop;
+        if (s + 2 * STEP <= s1 && lo >= 0 && hi <= pr.n) {
+          for (int64_t o = lo + t * 32; o < hi; o += P * 32) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(xr + o));
+            if constexpr (KIND == kFrameCross)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(pr.y + r * pr.ld_y + o));
+          }
+        }
+      }
       if constexpr (KIND == kFrameCross) {
         const float* yr = pr.y + r * pr.ld_y;
         float2 vy[E];

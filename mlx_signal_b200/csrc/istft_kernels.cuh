@@ -282,6 +282,12 @@ __global__ void __launch_bounds__(IstftHalfCfg<LOG_L, LOG_E>::THREADS)
     for (int s = f0; s < f1; s += 2) {
       const bool two = s + 1 < f1;
       const float2* za = zr + int64_t(s) * pr.ldf;
+      if (s + 3 < f1) {  // warm L2 with the next pair's two frames
+        const char* nx = reinterpret_cast<const char*>(za + 2 * int64_t(pr.ldf));
+        const int bytes = 2 * pr.ldf * 8;
+        for (int o = t * 128; o < bytes; o += P * 128)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + o));
+      }
       float2 v[E];
       istft_load_pair<PL>(v, za, za + pr.ldf, two, pr.nbins_in, t);
       team_pass0<PL>(v);
