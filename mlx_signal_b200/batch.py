@@ -142,6 +142,12 @@ def _tables(window, nperseg: int) -> _Tables | None:
     return hit
 
 
+def _batch_team(nperseg: int) -> int:
+    """Threads per FFT team of the batched kernel's class (16 points per thread at 256, else 32):
+    the number of low window-spectrum bins its constant-detrend correction can apply."""
+    return nperseg // (16 if nperseg == 256 else 32)
+
+
 def _rows_view(X: torch.Tensor) -> tuple[torch.Tensor, int]:
     rows = math.prod(X.shape[:-1]) if X.dim() > 1 else 1
     n = X.shape[-1]
@@ -212,7 +218,7 @@ def prepare_welch(x, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=No
     else:
         return None
     tb = _tables(window, nper)
-    if tb is None or (code == 1 and tb.wdft is None):
+    if tb is None or (code == 1 and (tb.wdft is None or tb.n_low > _batch_team(nper))):
         return None
     if scaling == "density":
         scale = 1.0 / (float(fs) * tb.sum_w2)

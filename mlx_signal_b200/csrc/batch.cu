@@ -13,7 +13,7 @@ namespace b2s {
 
 // Inter-pass twiddles of the 4096-point class, which do not fit the shared-memory union; built
 // once per device by k_batch_init (FP64 sincospi, rounded once, as the shared tables).
-using BatchPlan12 = Plan<12, team_log_e<12>()>;
+using BatchPlan12 = Plan<12, batch_log_e<12>()>;
 __device__ float2 g_batch_tw12[BatchPlan12::TW];
 
 __global__ void k_batch_init() {
@@ -59,10 +59,10 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) k_batch(BatchP
     const BatchReqDev* rq = reqs + ri;
     const int local = it - ldg_i(item_begin + ri);
     switch (ldg_i(&rq->log_l)) {
-      case 8: batch_item<8, team_log_e<8>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
-      case 9: batch_item<9, team_log_e<9>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
-      case 10: batch_item<10, team_log_e<10>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
-      case 12: batch_item<12, team_log_e<12>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
+      case 8: batch_item<8, batch_log_e<8>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
+      case 9: batch_item<9, batch_log_e<9>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
+      case 10: batch_item<10, batch_log_e<10>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
+      case 12: batch_item<12, batch_log_e<12>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
       default: break;  // rejected by the encoder
     }
     __syncthreads();
@@ -92,7 +92,7 @@ bool batch_class(int nperseg, int* log_l) {
 }
 
 int teams_of(int log_l) {
-  const int P = (1 << log_l) >> team_log_e_rt(log_l);
+  const int P = (1 << log_l) >> batch_log_e_rt(log_l);
   return P >= 64 ? 1 : kBatchThreads / P;
 }
 
@@ -131,7 +131,7 @@ int plan_request(const sp_batch_request& r, int idx, ReqPlan* p) {
                 "none/constant", idx);
       return SP_ERR_ARG;
     }
-    const int P = L >> team_log_e_rt(p->log_l);
+    const int P = L >> batch_log_e_rt(p->log_l);
     if (r.detrend == SP_DETREND_CONSTANT && (!r.win_dft_low || r.n_low < 1 || r.n_low > P)) {
       set_error("request %d: constant detrend needs 1 <= n_low <= %d window-spectrum bins", idx,
                 P);

@@ -13,18 +13,27 @@
 namespace b2s {
 
 // Points per thread for a team FFT of length 2^LOG_L: single-thread FFTs up to 32 points, then
-// teams of 8-128 threads with one register exchange for L = 256 and 1024.
+// teams of 8-64 threads with one register exchange for L = 256 and 1024; L = 4096 uses 16 points
+// on 256 threads (three radix-16 passes: a quarter of the registers of 32 points per thread, so
+// twice the resident warps).
 template <int LOG_L>
 constexpr int team_log_e() {
-  return LOG_L <= 5 ? LOG_L : (LOG_L == 6 ? 3 : (LOG_L <= 8 ? 4 : 5));
+  return LOG_L <= 5 ? LOG_L : (LOG_L == 6 ? 3 : (LOG_L <= 8 ? 4 : (LOG_L == 12 ? 4 : 5)));
+}
+
+// Points per thread of the batched kernel's classes (128-thread CTAs: 32 points at L = 4096).
+template <int LOG_L>
+constexpr int batch_log_e() {
+  return LOG_L == 12 ? 5 : team_log_e<LOG_L>();
 }
 
 constexpr int kMaxLogL = 12;
 
 // Runtime twin of team_log_e.
 inline int team_log_e_rt(int log_l) {
-  return log_l <= 5 ? log_l : (log_l == 6 ? 3 : (log_l <= 8 ? 4 : 5));
+  return log_l <= 5 ? log_l : (log_l == 6 ? 3 : (log_l <= 8 ? 4 : (log_l == 12 ? 4 : 5)));
 }
+inline int batch_log_e_rt(int log_l) { return log_l == 12 ? 5 : team_log_e_rt(log_l); }
 
 template <class P>
 using LaunchFnT = void (*)(dim3, int, size_t, cudaStream_t, const P&);
