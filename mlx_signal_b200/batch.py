@@ -143,9 +143,9 @@ def _tables(window, nperseg: int) -> _Tables | None:
 
 
 def _batch_team(nperseg: int) -> int:
-    """Threads per FFT team of the batched kernel's class (16 points per thread at 256, else 32):
-    the number of low window-spectrum bins its constant-detrend correction can apply."""
-    return nperseg // (16 if nperseg == 256 else 32)
+    """Threads per FFT team of the batched kernel's class (32 points per thread at 1024 and 4096,
+    16 at 256 and 512): the low window-spectrum bins its constant-detrend correction can apply."""
+    return nperseg // (32 if nperseg in (1024, 4096) else 16)
 
 
 def _rows_view(X: torch.Tensor) -> tuple[torch.Tensor, int]:

@@ -13,12 +13,12 @@
 namespace b2s {
 
 // Points per thread for a team FFT of length 2^LOG_L: single-thread FFTs up to 32 points, then
-// teams of 8-64 threads with one register exchange for L = 256 and 1024; L = 4096 uses 16 points
-// on 256 threads (three radix-16 passes: a quarter of the registers of 32 points per thread, so
-// twice the resident warps).
+// 16 points per thread (8 at L = 64), except L = 1024, whose 32 x 32 split needs one register
+// exchange. Measured on 64 x 2^20: 16 points beat 32 at L = 512, 2048 and 4096 (a quarter of the
+// registers, so twice the resident warps), and lose at L = 1024.
 template <int LOG_L>
 constexpr int team_log_e() {
-  return LOG_L <= 5 ? LOG_L : (LOG_L == 6 ? 3 : (LOG_L <= 8 ? 4 : (LOG_L == 12 ? 4 : 5)));
+  return LOG_L <= 5 ? LOG_L : (LOG_L == 6 ? 3 : (LOG_L == 10 ? 5 : 4));
 }
 
 // Points per thread of the batched kernel's classes (128-thread CTAs: 32 points at L = 4096).
@@ -31,7 +31,7 @@ constexpr int kMaxLogL = 12;
 
 // Runtime twin of team_log_e.
 inline int team_log_e_rt(int log_l) {
-  return log_l <= 5 ? log_l : (log_l == 6 ? 3 : (log_l <= 8 ? 4 : (log_l == 12 ? 4 : 5)));
+  return log_l <= 5 ? log_l : (log_l == 6 ? 3 : (log_l == 10 ? 5 : 4));
 }
 inline int batch_log_e_rt(int log_l) { return log_l == 12 ? 5 : team_log_e_rt(log_l); }
 

@@ -25,7 +25,7 @@ REQ_DT = np.dtype([
     ("pad0", "<i4"), ("scale", "<f4"), ("pad1", "<f4"),
 ])
 assert REQ_DT.itemsize == 144
-TEAMS = {8: 8, 9: 8, 10: 4, 12: 1}
+TEAMS = {8: 8, 9: 4, 10: 4, 12: 1}
 
 
 def welch_req(nperseg, rows, n, detrend=1, G=0, onesided=1, k=0):
