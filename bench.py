@@ -394,7 +394,11 @@ def secondary(x, steps, warmup, dist, clocks):
     b = 2 * C * NSAMP * 4 + C * NBINS * 4
     out["coherence_64x2p20"] = {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak}
     nseg = (NSAMP - NPERSEG) // HOP + 1
-    ms = timed(lambda: _kernels.frames("power", x, win_s, NPERSEG, NPERSEG, HOP, 1, True),
+    # hann + constant detrend: the public spectrogram applies the detrend as a spectral correction
+    low = _kernels.window_low_spectrum(win_s.cpu().numpy(), NPERSEG)
+    wd = torch.from_numpy(low[0]).to(x.device) if low is not None else None
+    ms = timed(lambda: _kernels.frames("power", x, win_s, NPERSEG, NPERSEG, HOP, 1, True,
+                                       wdft=wd),
                k, warmup, dist, clocks)
     b = C * NSAMP * 4 + C * nseg * NBINS * 4
     out["spectrogram_psd_64x2p20"] = {"ms": ms, "GB/s": b / ms / 1e6,

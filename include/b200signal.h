@@ -151,6 +151,22 @@ SP_API int sp_spectrogram_f32(const float* x, int64_t rows, int64_t n, int64_t l
                               void* stream);
 
 /*
+ * sp_stft_c64 / sp_spectrogram_f32 with the constant detrend (detrend == SP_DETREND_CONSTANT)
+ * applied after the transform as a correction on the window's non-zero low bins: win_dft_low
+ * holds DFT_nfft(win)[0..n_low) as complex (re, im); it is used when 1 <= n_low <=
+ * sp_welch_spectral_bins(nfft), otherwise the time-domain detrend runs. Same outputs as the plain
+ * entry points (scipy's detrend='constant': mean removed per segment before the window).
+ */
+SP_API int sp_stft_c64_ex(const float* x, int64_t rows, int64_t n, int64_t ld, int ext,
+                          int ext_mode, int64_t n_total, const float* win,
+                          const float* win_dft_low, int n_low, int nperseg, int nfft, int hop,
+                          int detrend, int onesided, float* out, void* stream);
+SP_API int sp_spectrogram_f32_ex(const float* x, int64_t rows, int64_t n, int64_t ld, int ext,
+                                 int ext_mode, int64_t n_total, const float* win,
+                                 const float* win_dft_low, int n_low, int nperseg, int nfft,
+                                 int hop, int detrend, int onesided, float* out, void* stream);
+
+/*
  * Per-frame cross spectra conj(X_s) Y_s, (rows, nseg, nbins) complex64, no one-sided factor.
  * Replaces _stft_metal.csd_frames (_stft_metal.py:412-414), used for average='median'.
  */

@@ -132,12 +132,14 @@ EXT_CODES = {None: 0, "zeros": 1, "even": 2, "odd": 3, "constant": 4}
 
 def frames(kind: str, x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop: int,
            detrend: int, onesided: bool, ext: int = 0, ext_mode=None, n_total: int | None = None,
-           y: torch.Tensor | None = None) -> torch.Tensor:
+           y: torch.Tensor | None = None, wdft: torch.Tensor | None = None) -> torch.Tensor:
     """Per-frame spectra of each row: (rows, nseg, nbins).
 
     kind 'stft' -> complex64 X_s; 'power' -> float32 |X_s|^2 with one-sided doubling;
     'cross' -> complex64 conj(X_s) Y_s (no doubling). Boundary extension (`ext` samples per
     side, scipy `boundary` mode `ext_mode`) and zero padding up to `n_total` are virtual.
+    `wdft` (optional, complex64 CUDA, DFT_nfft(win) low bins): with detrend 1 (constant) the mean
+    is removed as a spectral correction after the transform (stft / power only).
     """
     x, ldx = _rows(x)
     rows, n = x.shape
@@ -145,14 +147,30 @@ def frames(kind: str, x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: in
     nseg = (n_total - nperseg) // hop + 1
     nbins = nfft // 2 + 1 if onesided else nfft
     lib = _lib.load()
+    spec = wdft is not None and detrend == 1 and kind in ("power", "stft")
     if kind == "power":
         out = torch.empty((rows, nseg, nbins), dtype=torch.float32, device=x.device)
+        if spec:
+            _lib.check(lib.sp_spectrogram_f32_ex(x.data_ptr(), rows, n, ldx, ext,
+                                                 EXT_CODES[ext_mode], n_total, win.data_ptr(),
+                                                 wdft.data_ptr(), wdft.numel(), nperseg, nfft, hop,
+                                                 detrend, int(onesided), out.data_ptr(),
+                                                 stream_handle()),
+                       "sp_spectrogram_f32_ex")
+            return out
         _lib.check(lib.sp_spectrogram_f32(x.data_ptr(), rows, n, ldx, ext, EXT_CODES[ext_mode],
                                           n_total, win.data_ptr(), nperseg, nfft, hop, detrend,
                                           int(onesided), out.data_ptr(), stream_handle()),
                    "sp_spectrogram_f32")
         return out
     out = torch.empty((rows, nseg, nbins), dtype=torch.complex64, device=x.device)
+    if kind == "stft" and spec:
+        _lib.check(lib.sp_stft_c64_ex(x.data_ptr(), rows, n, ldx, ext, EXT_CODES[ext_mode],
+                                      n_total, win.data_ptr(), wdft.data_ptr(), wdft.numel(),
+                                      nperseg, nfft, hop, detrend, int(onesided), out.data_ptr(),
+                                      stream_handle()),
+                   "sp_stft_c64_ex")
+        return out
     if kind == "stft":
         _lib.check(lib.sp_stft_c64(x.data_ptr(), rows, n, ldx, ext, EXT_CODES[ext_mode], n_total,
                                    win.data_ptr(), nperseg, nfft, hop, detrend, int(onesided),

@@ -7,7 +7,11 @@
 namespace b2s {
 namespace {
 
-FrameInfo lookup(int kind, int log_l, int det) {
+FrameInfo lookup(int kind, int log_l, int det, bool spectral) {
+  if (spectral) {
+    return kind == kFrameStft ? frame_lookup_stft_spectral(log_l)
+                              : frame_lookup_power_spectral(log_l);
+  }
   if (kind == kFrameStft) return frame_lookup_stft(log_l, det);
   if (kind == kFramePower) return frame_lookup_power(log_l, det);
   return frame_lookup_cross(log_l, det);
@@ -16,7 +20,7 @@ FrameInfo lookup(int kind, int log_l, int det) {
 int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
                int64_t ldy, int ext, int ext_mode, int64_t n_total, const float* win,
                int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
-               void* stream) {
+               void* stream, const float* wdft = nullptr, int n_low = 0) {
   if (!x || !win || !out || (kind == kFrameCross && !y) || ldx < n ||
       (kind == kFrameCross && ldy < n)) {
     set_error("null pointer or row stride smaller than n");
@@ -35,7 +39,11 @@ int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n
     set_error("nfft=%d: fused kernels need a power of two <= %d", nfft, 1 << kMaxLogL);
     return SP_ERR_UNSUPPORTED;
   }
-  const FrameInfo f = lookup(kind, log_l, detrend);
+  // the spectral correction applies to the constant detrend when the window's spectrum is
+  // confined to bins a team thread holds in its first and last register
+  const bool spectral = kind != kFrameCross && detrend == kDetrendConstant && wdft != nullptr &&
+                        n_low >= 1 && n_low <= ((1 << log_l) >> team_log_e_rt(log_l));
+  const FrameInfo f = lookup(kind, log_l, detrend, spectral);
   const int nseg = int((n_total - nperseg) / hop + 1);
   const int64_t total = rows * nseg;
   if (total == 0) return SP_OK;
@@ -70,6 +78,8 @@ int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n
   p.out = out;
   p.out2 = nullptr;
   p.out3 = nullptr;
+  p.wdft = spectral ? reinterpret_cast<const float2*>(wdft) : nullptr;
+  p.n_low = spectral ? n_low : 0;
   f.launch(dim3(unsigned(blocks)), f.threads, f.smem, static_cast<cudaStream_t>(stream), p);
   B2S_CHECK_CUDA(cudaGetLastError(), "frame kernel launch");
   return SP_OK;
@@ -85,6 +95,24 @@ int sp_stft_c64(const float* x, int64_t rows, int64_t n, int64_t ld, int ext, in
                 int onesided, float* out, void* stream) {
   return b2s::run_frames(b2s::kFrameStft, x, nullptr, rows, n, ld, 0, ext, ext_mode, n_total,
                          win, nperseg, nfft, hop, detrend, onesided, out, stream);
+}
+
+int sp_stft_c64_ex(const float* x, int64_t rows, int64_t n, int64_t ld, int ext, int ext_mode,
+                   int64_t n_total, const float* win, const float* win_dft_low, int n_low,
+                   int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
+                   void* stream) {
+  return b2s::run_frames(b2s::kFrameStft, x, nullptr, rows, n, ld, 0, ext, ext_mode, n_total,
+                         win, nperseg, nfft, hop, detrend, onesided, out, stream, win_dft_low,
+                         n_low);
+}
+
+int sp_spectrogram_f32_ex(const float* x, int64_t rows, int64_t n, int64_t ld, int ext,
+                          int ext_mode, int64_t n_total, const float* win,
+                          const float* win_dft_low, int n_low, int nperseg, int nfft, int hop,
+                          int detrend, int onesided, float* out, void* stream) {
+  return b2s::run_frames(b2s::kFramePower, x, nullptr, rows, n, ld, 0, ext, ext_mode, n_total,
+                         win, nperseg, nfft, hop, detrend, onesided, out, stream, win_dft_low,
+                         n_low);
 }
 
 int sp_spectrogram_f32(const float* x, int64_t rows, int64_t n, int64_t ld, int ext,

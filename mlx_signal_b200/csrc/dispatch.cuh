@@ -59,6 +59,8 @@ MeanInfo mean_lookup_cross(int log_l, int det);
 MeanInfo mean_lookup_welch_half(int log_l, int det);  // det 0/1/2(spectral), log_l >= 1
 FrameInfo frame_lookup_stft(int log_l, int det);
 FrameInfo frame_lookup_power(int log_l, int det);
+FrameInfo frame_lookup_stft_spectral(int log_l);   // constant detrend, spectral correction
+FrameInfo frame_lookup_power_spectral(int log_l);
 FrameInfo frame_lookup_cross(int log_l, int det);
 
 // Fold-expression lookup over LOG_L = 0..kMaxLogL and detrend 0..2 of an info factory.

@@ -62,12 +62,30 @@ __device__ __forceinline__ void load_frames(float2 (&v)[PL::E], const float* __r
   }
 }
 
+// Extra shared memory of the spectral-detrend frame kernels: the low-bin window spectrum
+// (2P complex) after the exchange buffers.
+template <class CFG>
+constexpr size_t frame_spectral_extra() {
+  return size_t(2 * CFG::PL::P) * 8;
+}
+
+// DET == kDetrendConstantSpectral: the constant detrend as a spectral correction. The two frames
+// of a pair share one FFT of z = x_s + i x_{s+1} (or x + i y for the cross kind), so
+// FFT(w (z - m)) = FFT(w z) - (m_s + i m_{s+1}) DFT(w): only the low bins where the window's
+// spectrum is non-zero (k < n_low, k > L - n_low) are corrected, after the transform.
 template <int LOG_L, int LOG_E, int DET, int KIND>
 __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS) k_frames(FrameParams pr) {
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
   constexpr int L = PL::L, E = PL::E, P = PL::P;
+  constexpr bool SPEC = DET == kDetrendConstantSpectral;
   const MeanSmem sm = mean_smem_setup<CFG>(pr.win, pr.nperseg);
+  float2* wlo = sm.buf + CFG::TEAMS * PL::BUF;
+  float2* whi = wlo + P;
+  if constexpr (SPEC) {
+    load_window_lowbins<P>(wlo, whi, pr.wdft, pr.n_low, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
   const int team = threadIdx.x / P, t = threadIdx.x - team * P;
   const unsigned mask = team_mask<P>();
   float4* scratch = sm.scratch + team * CFG::SCRATCH;
@@ -112,9 +130,23 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS) k_frames(Frame
       } else {
         load_frames<PL>(v, xr, pr.n, pr.ext, pr.ext_mode, sa, sa + pr.hop, two, t, pr.nperseg);
       }
-      detrend_window<PL, DET>(v, sm.win, t, pr.nperseg, scratch, mask);
+      float2 m = make_float2(0.f, 0.f);
+      if constexpr (SPEC) {
+        const float sa = tree_sum<E>([&](auto ec) { return v[decltype(ec)::value].x; });
+        const float sb = tree_sum<E>([&](auto ec) { return v[decltype(ec)::value].y; });
+        const float4 s4 = team_sum4<P>(make_float4(sa, sb, 0.f, 0.f), scratch, mask);
+        const float inv = 1.0f / float(pr.nperseg);
+        m = make_float2(s4.x * inv, s4.y * inv);
+        detrend_window<PL, kDetrendNone>(v, sm.win, t, pr.nperseg, scratch, mask);
+      } else {
+        detrend_window<PL, DET>(v, sm.win, t, pr.nperseg, scratch, mask);
+      }
       team_pass0<PL>(v);
       team_passes<PL>(v, buf, sm.tw, t, mask);
+      if constexpr (SPEC) {
+        v[0] = csub(v[0], cmul(m, wlo[t]));
+        v[E - 1] = csub(v[E - 1], cmul(m, whi[t]));
+      }
 #pragma unroll
       for (int e = 0; e < E; ++e) buf[PL::pad(t + e * P)] = v[e];
       team_sync<P>(mask);

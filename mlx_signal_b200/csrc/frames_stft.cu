@@ -23,4 +23,27 @@ struct F {
 
 FrameInfo frame_lookup_stft(int log_l, int det) { return lookup_all<FrameInfo, F>(log_l, det); }
 
+namespace {
+// constant detrend as a low-bin spectral correction (DET = kDetrendConstantSpectral)
+template <int LOG_L, int UNUSED>
+struct FS {
+  static void launch(dim3 g, int t, size_t sm, cudaStream_t st, const FrameParams& p) {
+    k_frames<LOG_L, team_log_e<LOG_L>(), kDetrendConstantSpectral, kFrameStft><<<g, t, sm, st>>>(p);
+  }
+  static FrameInfo get() {
+    using CFG = MeanCfg<LOG_L, team_log_e<LOG_L>()>;
+    FrameInfo k;
+    k.fn = reinterpret_cast<const void*>(
+        &k_frames<LOG_L, team_log_e<LOG_L>(), kDetrendConstantSpectral, kFrameStft>);
+    k.threads = CFG::THREADS;
+    k.smem = CFG::SMEM + frame_spectral_extra<CFG>();
+    k.teams = CFG::TEAMS;
+    k.launch = &launch;
+    return k;
+  }
+};
+}  // namespace
+
+FrameInfo frame_lookup_stft_spectral(int log_l) { return lookup_all<FrameInfo, FS>(log_l, 0); }
+
 }  // namespace b2s

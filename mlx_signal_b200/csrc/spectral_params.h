@@ -44,6 +44,8 @@ struct FrameParams {
   float* out;          // (rows, nseg, nbins) complex interleaved, or power
   float* out2;         // second output (per-frame pyy for coherence frames), else nullptr
   float* out3;         // third output (per-frame pxy), else nullptr
+  const float2* wdft;  // DFT_nfft(win)[0..n_low) for the spectral constant detrend, else nullptr
+  int n_low;
 };
 
 }  // namespace b2s

@@ -283,10 +283,11 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
 _WDFT_CACHE: dict = {}
 
 
-def _spectral_detrend_table(s):
+def _spectral_detrend_table(s, frames: bool = False):
     """Low-bin window spectrum (device complex64) enabling the constant detrend as a spectral
-    correction in the fused welch kernel, or None (time-domain detrend)."""
-    if s.code != 1 or s.nperseg != s.nfft or 2 * s.nstep != s.nperseg:
+    correction in the fused welch kernel (50% overlap, nperseg == nfft) or, with frames=True, in
+    the per-frame kernels (any overlap and nfft); None -> time-domain detrend."""
+    if s.code != 1 or (not frames and (s.nperseg != s.nfft or 2 * s.nstep != s.nperseg)):
         return None
     w32 = (s.win_np * np.sqrt(s.scale)).astype(np.float32)
     key = (w32.tobytes(), s.nfft)
@@ -500,7 +501,8 @@ def _frames_result(s, mode: str) -> torch.Tensor:
         n = X.shape[-1]
         res = _kernels.frames("power" if mode == "psd" else "stft", X.reshape(rows, n), s.win,
                               s.nperseg, s.nfft, s.nstep, s.code, s.onesided, ext=s.ext,
-                              ext_mode=s.boundary, n_total=s.n_total)
+                              ext_mode=s.boundary, n_total=s.n_total,
+                              wdft=_spectral_detrend_table(s, frames=True))
         return res.reshape(outer + res.shape[-2:])
     composed_path_notice("stft", "shape outside the fused kernels")
     X, _ = _materialize_frames_input(s)

@@ -246,3 +246,47 @@ def test_fused_istft_roundtrip_large(rng):
     _, x2 = msig.istft(z, nperseg=1024, noverlap=512)
     err = float((x2[:, : x.shape[1]].cpu() - torch.from_numpy(x)).abs().max())
     assert err < 1e-5 * float(np.abs(x).max()) * 10, err
+
+
+@pytest.mark.parametrize("nperseg,noverlap", [(64, 16), (256, 128), (1024, 768), (4096, 2048),
+                                              (512, 0)])
+@pytest.mark.parametrize("mode", ["psd", "stft"])
+def test_spectral_detrend_frames_match_scipy(rng, nperseg, noverlap, mode):
+    """Constant detrend applied as a low-bin spectral correction in the frame kernels (hann
+    window: three non-zero DFT bins), on data with a large DC offset, against float64 scipy and
+    against the time-domain detrend kernels."""
+    from mlx_signal_b200 import _kernels
+
+    x = (rng.standard_normal((3, 20000)) + 5.0).astype(np.float32)
+    if mode == "psd":
+        f_ref, t_ref, s_ref = sps.spectrogram(x.astype(np.float64), window="hann",
+                                              nperseg=nperseg, noverlap=noverlap)
+        f, t, s = msig.spectrogram(x, window="hann", nperseg=nperseg, noverlap=noverlap)
+    else:
+        f_ref, t_ref, s_ref = sps.stft(x.astype(np.float64), window="hann", nperseg=nperseg,
+                                       noverlap=noverlap, detrend="constant")
+        f, t, s = msig.stft(x, window="hann", nperseg=nperseg, noverlap=noverlap,
+                            detrend="constant")
+    assert tuple(s.shape) == s_ref.shape
+    assert_close(s, s_ref, rtol=1e-4, atol_frac=1e-5)
+    # same frames through the time-domain detrend kernel
+    win = msig.spectral.device_vector(
+        (msig.windows._window_np("hann", nperseg)
+         * (np.sqrt(1.0 / (msig.windows._window_np("hann", nperseg) ** 2).sum()) if mode == "psd"
+            else 1.0 / msig.windows._window_np("hann", nperseg).sum())).astype(np.float32))
+    hop = nperseg - noverlap
+    ext = nperseg // 2 if mode == "stft" else 0
+    n_ext = x.shape[1] + 2 * ext
+    n_total = n_ext + ((-(n_ext - nperseg) % hop) % nperseg if mode == "stft" else 0)
+    kind = "power" if mode == "psd" else "stft"
+    low = _kernels.window_low_spectrum(win.cpu().numpy(), nperseg)
+    assert low is not None
+    wd = torch.from_numpy(low[0]).cuda()
+    xt = torch.from_numpy(x).cuda()
+    a = _kernels.frames(kind, xt, win, nperseg, nperseg, hop, 1, True, ext=ext,
+                        ext_mode="zeros" if ext else None, n_total=n_total, wdft=wd)
+    b = _kernels.frames(kind, xt, win, nperseg, nperseg, hop, 1, True, ext=ext,
+                        ext_mode="zeros" if ext else None, n_total=n_total)
+    # both detrend forms carry an error ~ eps * |mean| * |DFT(w)_0| on the lowest bins (the
+    # spectral one from cancellation in the DC bin, the time-domain one from the rounded mean)
+    assert float((a - b).abs().max()) <= 1e-5 * float(b.abs().max())
