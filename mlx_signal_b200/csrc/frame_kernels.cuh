@@ -74,7 +74,8 @@ constexpr size_t frame_spectral_extra() {
 // FFT(w (z - m)) = FFT(w z) - (m_s + i m_{s+1}) DFT(w): only the low bins where the window's
 // spectrum is non-zero (k < n_low, k > L - n_low) are corrected, after the transform.
 template <int LOG_L, int LOG_E, int DET, int KIND>
-__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS) k_frames(FrameParams pr) {
+__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L, LOG_E>::MIN_CTAS)
+    k_frames(FrameParams pr) {
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
   constexpr int L = PL::L, E = PL::E, P = PL::P;

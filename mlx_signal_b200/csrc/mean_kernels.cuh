@@ -26,6 +26,9 @@ struct MeanCfg {
   using PL = Plan<LOG_L, LOG_E>;
   static constexpr int TEAMS = PL::P >= 64 ? 1 : 128 / PL::P;
   static constexpr int THREADS = TEAMS * PL::P;
+  // 128-thread CTAs held to 3 per SM (<= 168 registers); measured faster for the generic welch
+  // and the frame kernels, whose unbounded builds took ~208-254 registers (2 CTAs per SM)
+  static constexpr int MIN_CTAS = THREADS == 128 ? 3 : 1;
   static constexpr int SCRATCH = PL::P >= 64 ? PL::P / 32 : 1;   // float4 per team
   static constexpr int WIN = (PL::L + 3) & ~3;                     // window floats (16 B multiple)
   static constexpr size_t SMEM = size_t(TEAMS) * SCRATCH * 16      // team scratch
@@ -105,7 +108,7 @@ __device__ __forceinline__ void flush_mirror(float (&acc)[PL::E], float* dst, fl
 
 // Welch: partial[r][slot][k] = sum over the team's segments of |Z_k|^2, z = x_s + i x_{s+1}.
 template <int LOG_L, int LOG_E, int DET>
-__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
+__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L, LOG_E>::MIN_CTAS)
     k_welch_mean(MeanParams pr) {
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
