@@ -124,6 +124,23 @@ SP_API int sp_coherence_f32(const float* x, const float* y, int64_t rows, int64_
                      int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
                      float* out, void* workspace, size_t workspace_bytes, void* stream);
 
+/*
+ * sp_csd_c64 / sp_coherence_f32 with the constant detrend applied in the frequency domain, as
+ * sp_welch_f32_ex: win_dft_low = DFT_nfft(win)[0..n_low) (complex), used by the 50%-overlap
+ * kernels (nperseg == nfft == 2*hop) when detrend == SP_DETREND_CONSTANT and
+ * 1 <= n_low <= sp_welch_spectral_bins(nfft); otherwise identical to the plain entry points.
+ * Same workspace size (sp_mean_workspace_size kind 1). Same reference counterparts.
+ */
+SP_API int sp_csd_c64_ex(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+                         int64_t ldy, const float* win, const float* win_dft_low, int n_low,
+                         int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
+                         void* workspace, size_t workspace_bytes, void* stream);
+SP_API int sp_coherence_f32_ex(const float* x, const float* y, int64_t rows, int64_t n,
+                               int64_t ldx, int64_t ldy, const float* win,
+                               const float* win_dft_low, int n_low, int nperseg, int nfft,
+                               int hop, int detrend, float* out, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
 
 /* Boundary extension modes of the per-frame entry points (scipy stft `boundary`). */
 enum { SP_EXT_NONE = 0, SP_EXT_ZEROS = 1, SP_EXT_EVEN = 2, SP_EXT_ODD = 3, SP_EXT_CONSTANT = 4 };

@@ -93,9 +93,11 @@ def window_low_spectrum(win32, nfft: int):
 
 
 def cross_mean(mode: str, x: torch.Tensor, y: torch.Tensor, win: torch.Tensor, nperseg: int,
-               nfft: int, hop: int, detrend: int, onesided: bool = True) -> torch.Tensor:
+               nfft: int, hop: int, detrend: int, onesided: bool = True,
+               wdft: torch.Tensor | None = None) -> torch.Tensor:
     """mode 'csd': mean conj(X)Y (complex64, one-sided doubling if requested);
-    mode 'coherence': |Pxy|^2/(Pxx Pyy) (float32)."""
+    mode 'coherence': |Pxy|^2/(Pxx Pyy) (float32). `wdft`: as for welch_mean (constant detrend
+    as a spectral correction in the 50%-overlap kernels)."""
     x, ldx = _rows(x)
     y, ldy = _rows(y)
     assert x.shape == y.shape
@@ -108,6 +110,15 @@ def cross_mean(mode: str, x: torch.Tensor, y: torch.Tensor, win: torch.Tensor, n
     if mode == "csd":
         nout = nfft // 2 + 1 if onesided else nfft
         out = torch.empty((rows, nout), dtype=torch.complex64, device=x.device)
+        if wdft is not None:
+            _lib.check(
+                lib.sp_csd_c64_ex(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy, win.data_ptr(),
+                                  wdft.data_ptr(), wdft.numel(), nperseg, nfft, hop, detrend,
+                                  int(onesided), out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                  stream_handle()),
+                "sp_csd_c64_ex",
+            )
+            return out
         _lib.check(
             lib.sp_csd_c64(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy, win.data_ptr(),
                            nperseg, nfft, hop, detrend, int(onesided), out.data_ptr(),
@@ -117,6 +128,15 @@ def cross_mean(mode: str, x: torch.Tensor, y: torch.Tensor, win: torch.Tensor, n
         return out
     if mode == "coherence":
         out = torch.empty((rows, nfft // 2 + 1), dtype=torch.float32, device=x.device)
+        if wdft is not None:
+            _lib.check(
+                lib.sp_coherence_f32_ex(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy,
+                                        win.data_ptr(), wdft.data_ptr(), wdft.numel(), nperseg,
+                                        nfft, hop, detrend, out.data_ptr(), ws.data_ptr(),
+                                        ws.numel(), stream_handle()),
+                "sp_coherence_f32_ex",
+            )
+            return out
         _lib.check(
             lib.sp_coherence_f32(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy, win.data_ptr(),
                                  nperseg, nfft, hop, detrend, out.data_ptr(), ws.data_ptr(),

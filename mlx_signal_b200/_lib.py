@@ -47,6 +47,16 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         c_i,
         [c_fp, c_fp, c_i64, c_i64, c_i64, c_i64, c_fp, c_i, c_i, c_i, c_i, c_fp, c_p, c_sz, c_p],
     ),
+    "sp_csd_c64_ex": (
+        c_i,
+        [c_fp, c_fp, c_i64, c_i64, c_i64, c_i64, c_fp, c_fp, c_i, c_i, c_i, c_i, c_i, c_i, c_fp,
+         c_p, c_sz, c_p],
+    ),
+    "sp_coherence_f32_ex": (
+        c_i,
+        [c_fp, c_fp, c_i64, c_i64, c_i64, c_i64, c_fp, c_fp, c_i, c_i, c_i, c_i, c_i, c_fp, c_p,
+         c_sz, c_p],
+    ),
     "sp_stft_c64": (
         c_i,
         [c_fp, c_i64, c_i64, c_i64, c_i, c_i, c_i64, c_fp, c_i, c_i, c_i, c_i, c_i, c_fp, c_p],

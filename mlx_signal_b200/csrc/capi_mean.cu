@@ -84,8 +84,13 @@ struct MeanPlanInfo {
 // bins k < P and k > L - P are the first and last register of every team thread.
 int spectral_bins(int log_l) { return (1 << log_l) >> team_log_e_rt(log_l); }
 
-int make_plan(bool cross, int64_t rows, int64_t n, int nperseg, int nfft, int hop, int detrend,
+// mode: 0 welch, 1 csd, 2 coherence. The segments-per-team split (and so the workspace size)
+// comes from one canonical kernel per family (the time-domain-detrend variant, coherence for the
+// cross family), so sp_mean_workspace_size, which knows neither the detrend form nor csd vs
+// coherence, sizes every variant's launch.
+int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop, int detrend,
               MeanPlanInfo* pl, bool spectral = false) {
+  const bool cross = mode != 0;
   if (rows < 0 || n < 1 || nperseg < 1 || nperseg > n || hop < 1 || hop > nperseg ||
       nfft < nperseg || detrend < 0 || detrend > 2 || n >= (int64_t(1) << 31)) {
     set_error("invalid spectral-mean arguments (rows=%lld n=%lld nperseg=%d nfft=%d hop=%d)",
@@ -97,20 +102,34 @@ int make_plan(bool cross, int64_t rows, int64_t n, int nperseg, int nfft, int ho
     set_error("nfft=%d: fused kernels need a power of two <= %d", nfft, 1 << kMaxLog);
     return SP_ERR_UNSUPPORTED;
   }
-  const bool half = !cross && log_l >= 1 && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
-  pl->k = cross ? mean_lookup_cross(log_l, detrend)
-                : (half ? mean_lookup_welch_half(log_l, (spectral && detrend == 1) ? 2 : detrend)
-                        : mean_lookup_welch(log_l, detrend));
+  const bool half = log_l >= 1 && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
+  const int hdet = (spectral && detrend == 1) ? 2 : detrend;  // lookup index: 2 = spectral
+  MeanInfo canon;
+  if (cross && half) {
+    pl->k = mean_lookup_cross_half(log_l, hdet, mode == 1);
+    canon = mean_lookup_cross_half(log_l, detrend, false);
+  } else if (cross) {
+    pl->k = canon = mean_lookup_cross(log_l, detrend);
+  } else if (half) {
+    pl->k = mean_lookup_welch_half(log_l, hdet);
+    canon = mean_lookup_welch_half(log_l, detrend);
+  } else {
+    pl->k = canon = mean_lookup_welch(log_l, detrend);
+  }
   pl->log_l = log_l;
   pl->nseg = int((n - nperseg) / hop + 1);
   pl->total = rows * pl->nseg;
   int sms = 0;
-  const int nb = resident_ctas(pl->k.fn, pl->k.threads, pl->k.smem, &sms);
+  const int nb = resident_ctas(canon.fn, canon.threads, canon.smem, &sms);
+  if (resident_ctas(pl->k.fn, pl->k.threads, pl->k.smem, &sms) <= 0) {
+    set_error("no resident CTA for spectral-mean kernel (nfft=%d, smem=%zu)", nfft, pl->k.smem);
+    return SP_ERR_UNSUPPORTED;
+  }
   if (nb <= 0) {
     set_error("no resident CTA for spectral-mean kernel (nfft=%d, smem=%zu)", nfft, pl->k.smem);
     return SP_ERR_UNSUPPORTED;
   }
-  const int64_t cap = int64_t(nb) * sms * pl->k.teams;
+  const int64_t cap = int64_t(nb) * sms * canon.teams;
   const int64_t total = pl->total > 0 ? pl->total : 1;
   pl->G = cross ? cdiv(total, cap) : 2 * cdiv(total, 2 * cap);
   if (pl->G < 1) pl->G = 1;
@@ -135,10 +154,10 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
     return SP_ERR_ARG;
   }
   const int log_l_in = ilog2_exact(nfft);
-  const bool spectral = !cross && wdft != nullptr && n_low >= 1 && log_l_in >= 1 &&
+  const bool spectral = wdft != nullptr && n_low >= 1 && log_l_in >= 1 &&
                         n_low <= spectral_bins(log_l_in);
   MeanPlanInfo pl;
-  int st = make_plan(cross, rows, n, nperseg, nfft, hop, detrend, &pl, spectral);
+  int st = make_plan(mode, rows, n, nperseg, nfft, hop, detrend, &pl, spectral);
   if (st != SP_OK) return st;
   if (rows == 0) return SP_OK;
   if (ws_bytes < size_t(pl.ws_bytes) || (pl.ws_bytes > 0 && !ws)) {
@@ -161,6 +180,7 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   p.cmax = pl.cmax;
   p.total = pl.total;
   p.partial = static_cast<float*>(ws);
+  // the spectral tables are read only by the 50%-overlap kernels' spectral variants
   p.wdft = spectral ? reinterpret_cast<const float2*>(wdft) : nullptr;
   p.n_low = spectral ? n_low : 0;
   pl.k.launch(dim3(unsigned(pl.blocks)), pl.k.threads, pl.k.smem, s, p);
@@ -238,7 +258,7 @@ int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld, co
                          int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
                          void* stream) {
   b2s::MeanPlanInfo pl;
-  const int st = b2s::make_plan(false, rows, n, nperseg, nfft, hop, detrend, &pl);
+  const int st = b2s::make_plan(0, rows, n, nperseg, nfft, hop, detrend, &pl);
   if (st != SP_OK) return st;
   if (size_t(pl.ws_bytes) > b2s::kNoAllocScratchBytes) {
     b2s::set_error(
@@ -257,7 +277,7 @@ int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld, co
 int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
                                int detrend) {
   b2s::MeanPlanInfo pl;
-  const int st = b2s::make_plan(kind != 0, rows, n, nperseg, nfft, hop, detrend, &pl);
+  const int st = b2s::make_plan(kind != 0 ? 2 : 0, rows, n, nperseg, nfft, hop, detrend, &pl);
   return st == SP_OK ? pl.ws_bytes : int64_t(st);
 }
 
@@ -287,6 +307,22 @@ int sp_csd_c64(const float* x, const float* y, int64_t rows, int64_t n, int64_t 
                int onesided, float* out, void* workspace, size_t workspace_bytes, void* stream) {
   return b2s::run_mean(1, x, y, rows, n, ldx, ldy, win, nperseg, nfft, hop, detrend, onesided,
                        out, workspace, workspace_bytes, stream);
+}
+
+int sp_csd_c64_ex(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+                  int64_t ldy, const float* win, const float* win_dft_low, int n_low, int nperseg,
+                  int nfft, int hop, int detrend, int onesided, float* out, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(1, x, y, rows, n, ldx, ldy, win, nperseg, nfft, hop, detrend, onesided,
+                       out, workspace, workspace_bytes, stream, win_dft_low, n_low);
+}
+
+int sp_coherence_f32_ex(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+                        int64_t ldy, const float* win, const float* win_dft_low, int n_low,
+                        int nperseg, int nfft, int hop, int detrend, float* out, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(2, x, y, rows, n, ldx, ldy, win, nperseg, nfft, hop, detrend, 1, out,
+                       workspace, workspace_bytes, stream, win_dft_low, n_low);
 }
 
 int sp_coherence_f32(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,

@@ -57,6 +57,7 @@ IstftInfo istft_half_lookup(int log_l);  // hop == nperseg / 2
 MeanInfo mean_lookup_welch(int log_l, int det);
 MeanInfo mean_lookup_cross(int log_l, int det);
 MeanInfo mean_lookup_welch_half(int log_l, int det);  // det 0/1/2(spectral), log_l >= 1
+MeanInfo mean_lookup_cross_half(int log_l, int det, bool csd);  // det 0/1/2(spectral)
 FrameInfo frame_lookup_stft(int log_l, int det);
 FrameInfo frame_lookup_power(int log_l, int det);
 FrameInfo frame_lookup_stft_spectral(int log_l);   // constant detrend, spectral correction

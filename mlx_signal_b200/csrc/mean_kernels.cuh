@@ -469,6 +469,176 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
   }
 }
 
+// 50%-overlap csd / coherence (nperseg == nfft == L, hop == L/2), z = x_s + i y_s per segment:
+// segment s = A | B where A is the previous segment's B. The window multiply is fused into the
+// first radix-2 stage (which pairs n with n + L/2, i.e. A with B), from the transposed window
+// table; the segment means come from the carried half-block sum plus the new one; the constant
+// detrend runs inside the fused stage (DET == kDetrendConstant) or as the low-bin spectral
+// correction Z_k -= (m_x + i m_y) DFT(win)_k (DET == kDetrendConstantSpectral); the next
+// half-block is prefetched into L2. Partial slots are those of k_cross_mean (Q_k for all k,
+// C_k = Z_k Z_{L-k} for k <= L/2); CSD accumulates only Im C (its real part is stored as zero:
+// csd does not read it).
+template <int LOG_L, int LOG_E, int DET, bool CSD>
+__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
+    k_cross_half(MeanParams pr) {
+  using CFG = MeanCfg<LOG_L, LOG_E>;
+  using PL = typename CFG::PL;
+  constexpr int L = PL::L, E = PL::E, P = PL::P, H = L / 2, EH = E / 2, EH1 = E / 2 + 1;
+  constexpr int R0 = PL::radix(0), B0 = E / R0;
+  constexpr bool WT = HalfWinT<PL>::USE;
+  extern __shared__ float4 smem[];
+  float* win1 = reinterpret_cast<float*>(smem + CFG::TEAMS * CFG::SCRATCH);
+  float2* wlo = reinterpret_cast<float2*>(win1 + HalfSmem<CFG>::WINF);
+  float2* whi = wlo + P;
+  float2* tw = whi + P;
+  float2* sbuf = tw + PL::TW;
+  if constexpr (WT) {
+    build_half_wint<PL>(win1, pr.win, threadIdx.x);
+  } else {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) win1[i] = pr.win[i];
+  }
+  if constexpr (DET == kDetrendConstantSpectral)
+    load_window_lowbins<P>(wlo, whi, pr.wdft, pr.n_low, threadIdx.x, blockDim.x);
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  pdl_trigger();
+  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+  const unsigned mask = team_mask<P>();
+  float4* scratch = smem + team * CFG::SCRATCH;
+  float2* buf = sbuf + team * PL::BUF;
+  const float4* wt = reinterpret_cast<const float4*>(win1) + t * (HalfWinT<PL>::WS / 4);
+  const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
+  int64_t g = tau * pr.G;
+  const int64_t gend = min(g + pr.G, pr.total);
+  const float inv_n = 1.0f / float(L);
+  float q[E];
+  float cr[EH1], ci[EH1];
+#pragma unroll
+  for (int e = 0; e < E; ++e) q[e] = 0.f;
+#pragma unroll
+  for (int e = 0; e < EH1; ++e) cr[e] = ci[e] = 0.f;
+  while (g < gend) {
+    const int64_t r = g / pr.nseg;
+    const int s0 = int(g - r * pr.nseg);
+    const int64_t lim = int64_t(s0) + (gend - g);
+    const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
+    const float* xr = pr.x + r * pr.ld_x;
+    const float* yr = pr.y + r * pr.ld_y;
+    float sax = 0.f, say = 0.f;  // sums of this segment's A half (the previous B)
+    bool have_a = false;
+    for (int s = s0; s < s1; ++s) {
+      const float* ax = xr + int64_t(s) * H;
+      const float* ay = yr + int64_t(s) * H;
+      if (s + 2 < s1) {  // warm L2 with the next segment's new half-block
+        for (int o = t * 32; o < H; o += P * 32) {
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(ax + 2 * H + o));
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(ay + 2 * H + o));
+        }
+      }
+      float Ax[EH], Ay[EH], Bx[EH], By[EH];
+      static_for<0, EH>([&](auto gc) {
+        constexpr int gi = decltype(gc)::value;
+        const int n = slot_elem<PL, 2 * gi>(t);
+        Ax[gi] = __ldg(ax + n);
+        Ay[gi] = __ldg(ay + n);
+        Bx[gi] = __ldg(ax + H + n);
+        By[gi] = __ldg(ay + H + n);
+      });
+      float mx = 0.f, my = 0.f;
+      if constexpr (DET == kDetrendConstant || DET == kDetrendConstantSpectral) {
+        float sb[2] = {tree_sum<EH>([&](auto gc) { return Bx[decltype(gc)::value]; }),
+                       tree_sum<EH>([&](auto gc) { return By[decltype(gc)::value]; })};
+        if (!have_a) {
+          float s4[4] = {tree_sum<EH>([&](auto gc) { return Ax[decltype(gc)::value]; }),
+                         tree_sum<EH>([&](auto gc) { return Ay[decltype(gc)::value]; }), sb[0],
+                         sb[1]};
+          team_sum<P, 4>(s4, scratch, mask);
+          sax = s4[0];
+          say = s4[1];
+          sb[0] = s4[2];
+          sb[1] = s4[3];
+        } else {
+          team_sum<P, 2>(sb, scratch, mask);
+        }
+        mx = (sax + sb[0]) * inv_n;
+        my = (say + sb[1]) * inv_n;
+        sax = sb[0];
+        say = sb[1];
+        have_a = true;
+      }
+      float2 v[E];
+      auto fuse = [&](auto gc, float wl, float wh) {
+        constexpr int gi = decltype(gc)::value;
+        float2 zl = make_float2(Ax[gi], Ay[gi]);
+        float2 zh = make_float2(Bx[gi], By[gi]);
+        if constexpr (DET == kDetrendConstant) {
+          zl = make_float2(zl.x - mx, zl.y - my);
+          zh = make_float2(zh.x - mx, zh.y - my);
+        }
+        const float2 a = make_float2(zl.x * wl, zl.y * wl);
+        v[2 * gi] = make_float2(fmaf(zh.x, wh, a.x), fmaf(zh.y, wh, a.y));
+        v[2 * gi + 1] = make_float2(fmaf(-zh.x, wh, a.x), fmaf(-zh.y, wh, a.y));
+      };
+      if constexpr (WT) {
+        static_for<0, EH / 2>([&](auto pc) {
+          constexpr int gp = decltype(pc)::value;
+          const float4 w4 = wt[gp];
+          fuse(std::integral_constant<int, 2 * gp>{}, w4.x, w4.y);
+          fuse(std::integral_constant<int, 2 * gp + 1>{}, w4.z, w4.w);
+        });
+      } else {
+        static_for<0, EH>([&](auto gc) {
+          constexpr int gi = decltype(gc)::value;
+          const int n = slot_elem<PL, 2 * gi>(t);
+          fuse(gc, win1[n], win1[n + H]);
+        });
+      }
+      static_for<0, B0>([&](auto bc) {
+        constexpr int b = decltype(bc)::value;
+        dft_dit<R0, b * R0, 2>(v);
+      });
+      team_passes<PL>(v, buf, tw, t, mask);
+      if constexpr (DET == kDetrendConstantSpectral) {
+        const float2 m = make_float2(mx, my);
+        v[0] = csub(v[0], cmul(m, wlo[t]));
+        v[E - 1] = csub(v[E - 1], cmul(m, whi[t]));
+      }
+      // |Z_k|^2 for every bin; Z_k Z_{L-k} for k <= L/2 through a mirror exchange
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        q[e] = fmaf(v[e].x, v[e].x, q[e]);
+        q[e] = fmaf(v[e].y, v[e].y, q[e]);
+        buf[PL::pad(t + e * P)] = v[e];
+      }
+      team_sync<P>(mask);
+#pragma unroll
+      for (int e = 0; e < EH1; ++e) {
+        if (e < E / 2 || t == 0) {
+          const int k = t + e * P;
+          const float2 m = buf[PL::pad((L - k) & (L - 1))];
+          if constexpr (!CSD) cr[e] = fmaf(v[e].x, m.x, fmaf(-v[e].y, m.y, cr[e]));
+          ci[e] = fmaf(v[e].x, m.y, fmaf(v[e].y, m.x, ci[e]));
+        }
+      }
+      team_sync<P>(mask);
+    }
+    const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
+    float* dst = pr.partial + (r * pr.cmax + slot) * int64_t(cross_slot_floats(L));
+    float2* dstc = reinterpret_cast<float2*>(dst + cross_q_floats(L));
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      dst[t + e * P] = q[e];
+      q[e] = 0.f;
+    }
+#pragma unroll
+    for (int e = 0; e < EH1; ++e) {
+      if (e < E / 2 || t == 0) dstc[t + e * P] = make_float2(CSD ? 0.f : cr[e], ci[e]);
+      cr[e] = ci[e] = 0.f;
+    }
+    g += s1 - s0;
+  }
+}
+
 // Final reduction over partial slots (fixed order, FP64), mirror combination, one-sided
 // doubling and 1/nseg. mode: 0 welch (float out), 1 csd (complex out), 2 coherence (float out).
 struct ReduceParams {

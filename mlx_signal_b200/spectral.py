@@ -289,11 +289,16 @@ def _spectral_detrend_table(s, frames: bool = False):
     the per-frame kernels (any overlap and nfft); None -> time-domain detrend."""
     if s.code != 1 or (not frames and (s.nperseg != s.nfft or 2 * s.nstep != s.nperseg)):
         return None
-    w32 = (s.win_np * np.sqrt(s.scale)).astype(np.float32)
-    key = (w32.tobytes(), s.nfft)
+    return _window_table((s.win_np * np.sqrt(s.scale)).astype(np.float32), s.nfft)
+
+
+def _window_table(w32: np.ndarray, nfft: int):
+    """Cached device complex64 DFT_nfft(w32) low bins, or None when the window's spectrum is not
+    confined to bins the kernels can correct."""
+    key = (w32.tobytes(), nfft)
     hit = _WDFT_CACHE.get(key, False)
     if hit is False:
-        low = _kernels.window_low_spectrum(w32, s.nfft)
+        low = _kernels.window_low_spectrum(w32, nfft)
         hit = None if low is None else device_vector(low[0], dtype=torch.complex64)
         if len(_WDFT_CACHE) >= 64:
             _WDFT_CACHE.clear()
@@ -365,7 +370,7 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
             Xb = X.expand(outer + (n,)).reshape(rows, n)
             Yb = Y.expand(outer + (n,)).reshape(rows, n)
             res = _kernels.cross_mean("csd", Xb, Yb, s.win, s.nperseg, s.nfft, s.nstep, s.code,
-                                      s.onesided)
+                                      s.onesided, wdft=_spectral_detrend_table(s))
         pxy = res.reshape(outer + (res.shape[-1],))
     else:
         rows = int(np.prod(outer)) if outer else 1
@@ -474,9 +479,12 @@ def coherence(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=Non
             outer = tuple(X.shape[:-1])
             rows = int(np.prod(outer)) if outer else 1
             n = X.shape[-1]
-            win = device_vector(win_np.astype(np.float32))
+            win32 = win_np.astype(np.float32)
+            win = device_vector(win32)
+            wdft = (_window_table(win32, nft)
+                    if code == 1 and nps == nft and 2 * (nps - nov) == nps else None)
             cxy = _kernels.cross_mean("coherence", X.reshape(rows, n), Y.reshape(rows, n), win,
-                                      nps, nft, nps - nov, code)
+                                      nps, nft, nps - nov, code, wdft=wdft)
             cxy = cxy.reshape(outer + (cxy.shape[-1],))
             if cxy.dim() > 1 and ax != cxy.dim() - 1:
                 cxy = cxy.movedim(-1, ax)

@@ -260,3 +260,30 @@ def test_spectral_and_time_domain_detrend_agree(rng):
     b = _kernels.welch_mean(x, wt, nper, nper, nper // 2, 1, True,
                             wdft=torch.from_numpy(low[0]).cuda())
     torch.testing.assert_close(a, b, rtol=2e-5, atol=1e-6 * float(a.max()))
+
+
+@pytest.mark.parametrize("nperseg", [16, 64, 256, 512, 1024, 2048, 4096])
+@pytest.mark.parametrize("detrend", ["constant", False])
+def test_half_overlap_cross_spectra_match_scipy(rng, nperseg, detrend):
+    """50%-overlap csd / coherence (the fused half-block kernel: window in the first butterfly
+    stage, spectral or time-domain constant detrend) against float64 scipy, with a DC offset."""
+    from mlx_signal_b200 import _kernels
+
+    n = 40 * nperseg
+    x = (rng.standard_normal((3, n)) + 2.0).astype(np.float32)
+    y = (0.6 * np.roll(x, 7, axis=-1) + 0.4 * rng.standard_normal((3, n)) - 1.0).astype(np.float32)
+    kw = dict(nperseg=nperseg, fs=100.0, detrend=detrend)
+    _, c_ref = sps.csd(x.astype(np.float64), y.astype(np.float64), **kw)
+    _, c = msig.csd(x, y, **kw)
+    assert rel_err_bins(c, c_ref) <= 1e-5
+    _, h_ref = sps.coherence(x.astype(np.float64), y.astype(np.float64), **kw)
+    _, h = msig.coherence(x, y, **kw)
+    assert_close(h, h_ref, rtol=1e-4, atol_frac=1e-5)
+    if detrend == "constant":  # the time-domain detrend variant of the same kernel
+        w = msig.spectral.device_vector(
+            (msig.windows._window_np("hann", nperseg)
+             * np.sqrt(1.0 / (100.0 * (msig.windows._window_np("hann", nperseg) ** 2).sum())))
+            .astype(np.float32))
+        ct = _kernels.cross_mean("csd", torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(), w,
+                                 nperseg, nperseg, nperseg // 2, 1, True)
+        assert rel_err_bins(ct, c_ref) <= 1e-5
