@@ -338,7 +338,7 @@ __device__ __forceinline__ void load_window_lowbins(float2* lo, float2* hi, cons
 }
 
 template <int LOG_L, int LOG_E, int DET>
-__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
+__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L, LOG_E>::MIN_CTAS)
     k_welch_half(MeanParams pr) {
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
 // C_k = Z_k Z_{L-k} for k <= L/2); CSD accumulates only Im C (its real part is stored as zero:
 // csd does not read it).
 template <int LOG_L, int LOG_E, int DET, bool CSD>
-__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
+__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L, LOG_E>::MIN_CTAS)
     k_cross_half(MeanParams pr) {
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
