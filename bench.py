@@ -370,6 +370,31 @@ def serving_sweep(seconds, rates=(1000, 5000, 10000, 20000, 50000, 100000, 20000
     return out
 
 
+def cpu_row_rate(fn_name, arrays, bytes_per_row, repeats=2, **kw):
+    """The reference's CPU route (scipy.signal through oracle.cpu_reference) on a row sample over
+    a spawn process pool of every host core: (GB/s of algorithmic bytes, cores, rows)."""
+    from oracle import cpu_reference
+
+    cores = os.cpu_count() or 1
+    rows = arrays[0].shape[0]
+    cpu_reference.pool_map_rows(fn_name, tuple(a[: min(rows, cores)] for a in arrays), cores, **kw)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        cpu_reference.pool_map_rows(fn_name, arrays, cores, **kw)
+        times.append(time.perf_counter() - t0)
+    return bytes_per_row * rows / statistics.median(times) / 1e9, cores, rows
+
+
+def with_cpu(entry, rate):
+    gbs, cores, rows = rate
+    entry["cpu_baseline"] = {"GB/s": gbs, "cores": cores, "kind": "port",
+                             "sample": f"{rows} of {C} channels, scipy.signal on float32 "
+                                       f"over a {cores}-process pool"}
+    entry["speedup_vs_cpu"] = entry["GB/s"] / gbs
+    return entry
+
+
 def secondary(x, steps, warmup, dist, clocks):
     """Cheaper side measurements of the other configs (device-resident inputs)."""
     import torch
@@ -433,6 +458,26 @@ def secondary(x, steps, warmup, dist, clocks):
     b = C * nseg_s * NBINS * 8 + C * NSAMP * 4
     out["istft_64x2p20"] = {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
                             "roundtrip_max_err_rel_peak": rt}
+    # the reference's CPU route on a channel sample, beside each GPU figure (rank 0, N = 1)
+    if dist is None:
+        ncpu = min(C, os.cpu_count() or 1)
+        xs = x[:ncpu].cpu().numpy()
+        ys = y[:ncpu].cpu().numpy()
+        kw = dict(fs=FS, nperseg=NPERSEG, noverlap=NOVERLAP)
+        with_cpu(out["csd_64x2p20"], cpu_row_rate("csd", (xs, ys), 2 * NSAMP * 4 + NBINS * 8, **kw))
+        with_cpu(out["coherence_64x2p20"],
+                 cpu_row_rate("coherence", (xs, ys), 2 * NSAMP * 4 + NBINS * 4, **kw))
+        with_cpu(out["spectrogram_psd_64x2p20"],
+                 cpu_row_rate("spectrogram", (xs,), NSAMP * 4 + nseg * NBINS * 4,
+                              window="hann", **kw))
+        with_cpu(out["stft_64x2p20"],
+                 cpu_row_rate("stft", (xs,), NSAMP * 4 + nseg_s * NBINS * 8, window="hann", **kw))
+        zs = z[:ncpu].transpose(1, 2).contiguous().cpu().numpy()  # (rows, nfreq, nseg)
+        with_cpu(out["istft_64x2p20"],
+                 cpu_row_rate("istft", (zs,), nseg_s * NBINS * 8 + NSAMP * 4, window="hann", **kw))
+        from oracle import cpu_reference
+
+        cpu_reference.close_pool()
     del y, z, xr
     out["batched_512_uneven"] = batched_uneven(dist, clocks, peak)
     out["rfft_1x2p23"] = large_rfft(dist, clocks, peak)
@@ -553,11 +598,21 @@ def large_rfft(dist, clocks, peak, log_n=23, seed=5):
                    "sp_rfft_c64")
 
     ms = timed(step, 20, 3, dist, clocks)
-    ref = np.fft.rfft(x.double().cpu().numpy())
+    xh = x.cpu().numpy()
+    ref = np.fft.rfft(xh.astype(np.float64))
     err = float(np.max(np.abs(X.cpu().numpy() - ref)) / np.max(np.abs(ref)))
     b = n * 4 + (n // 2 + 1) * 8
+    t_cpu = []
+    for _ in range(3):  # numpy.fft.rfft on float32, one transform on one core
+        t0 = time.perf_counter()
+        np.fft.rfft(xh)
+        t_cpu.append(time.perf_counter() - t0)
+    cpu = b / statistics.median(t_cpu) / 1e9
     return {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
-            "max_abs_err_rel_peak_vs_numpy_f64": err, "launches": 4}
+            "max_abs_err_rel_peak_vs_numpy_f64": err, "launches": 4,
+            "cpu_baseline": {"GB/s": cpu, "cores": 1, "kind": "port",
+                             "sample": "the full 2^23 transform, numpy.fft.rfft"},
+            "speedup_vs_cpu": b / ms / 1e6 / cpu}
 
 
 def run_ours(args, rank, world, local_rank, dist):
