@@ -15,6 +15,9 @@ from ._config import (
     set_config,
 )
 from . import fft
+from .convolution import fftconvolve, oaconvolve
+from .filtering import hilbert
+from .resampling import resample
 from .spectral import coherence, csd, istft, periodogram, spectrogram, stft, welch
 from .windows import get_window
 
@@ -28,10 +31,14 @@ __all__ = [
     "config_context",
     "csd",
     "fft",
+    "fftconvolve",
     "get_config",
     "get_window",
+    "hilbert",
     "istft",
+    "oaconvolve",
     "periodogram",
+    "resample",
     "set_config",
     "spectrogram",
     "stft",

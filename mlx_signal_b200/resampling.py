@@ -1,0 +1,119 @@
+"""Fourier-method resampling over the long FFTs (scipy.signal.resample semantics).
+
+Counterpart of the reference's `resample` (src/mlx_signal_processing/resampling.py:60-176), which
+follows scipy 1.18's algorithm: transform, optional frequency-domain window (named windows in
+fftshift order; a real input's one-sided spectrum takes the window folded onto itself), keep the
+m = min(num, n) lowest-frequency bins, split (upsampling) or join (downsampling) the unpaired
+bin at m/2 when m is even, scale by num / n and inverse-transform to num samples. Transforms run
+on the three-pass kernels where `mlx_signal_b200.fft` covers their length, cuFFT otherwise.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import fft as _fft
+from ._array import device, to_device, to_numpy
+from .windows import _window_np
+
+__all__ = ["resample"]
+
+
+def _freq_window(window, n: int) -> np.ndarray:
+    """Frequency-domain window values in fftfreq order (float64 or complex128)."""
+    if callable(window):
+        w = np.asarray(window(np.fft.fftfreq(n)))
+        if w.shape != (n,):
+            raise ValueError(f"window function returned shape {w.shape}, expected ({n},)")
+    elif isinstance(window, str | tuple):
+        w = np.fft.fftshift(_window_np(tuple(window) if isinstance(window, tuple) else window, n))
+    else:
+        w = np.asarray(to_numpy(window))
+        if w.shape != (n,):
+            raise ValueError(f"window.shape={w.shape} != ({n},), i.e., window length is not "
+                             "equal to number of frequency bins!")
+    return np.array(w, dtype=np.complex128 if np.iscomplexobj(w) else np.float64)
+
+
+def _dev(vals: np.ndarray) -> torch.Tensor:
+    dt = torch.complex64 if np.iscomplexobj(vals) else torch.float32
+    return torch.from_numpy(np.ascontiguousarray(vals)).to(device(), dtype=dt)
+
+
+def resample(x, num, t=None, axis=0, window=None, domain="time"):
+    """Resample x to num samples along `axis` with the Fourier method. Returns the resampled
+    signal, or (resampled, new_t) when sample positions t are given."""
+    if domain not in ("time", "freq"):
+        raise ValueError(f"Parameter {domain=} not in ('time', 'freq')!")
+    num = int(num)
+    X0 = to_device(x)
+    moved = X0.dim() > 1 and axis not in (-1, X0.dim() - 1)
+    xa = X0.movedim(axis, -1) if moved else X0
+    n = xa.shape[-1]
+    s_fac = n / num
+    m = min(num, n)
+    m2 = m // 2 + 1
+    W = None if window is None else _freq_window(window, n)
+    if domain == "time" and not xa.is_complex():
+        X = _fft.rfft(xa, axis=-1)
+        nX = X.shape[-1]
+        if W is not None:
+            Wf = W.copy()
+            Wf[1:nX] += np.flip(Wf[-nX + 1:]) if nX > 1 else 0
+            Wf[1:nX] /= 2
+            X = X * _dev(Wf[:nX])
+        X = X[..., :m2]
+        if m % 2 == 0 and num != n:  # the unpaired bin at m/2
+            fac = np.ones(m2, dtype=np.float32)
+            fac[m // 2] = 2.0 if num < n else 0.5
+            X = X * _dev(fac)
+        if W is not None and np.iscomplexobj(W):  # irfft reads DC (and Nyquist) as real
+            X = X.clone()
+            X[..., 0] = X[..., 0].real.to(torch.complex64)
+            if num % 2 == 0 and X.shape[-1] == num // 2 + 1:
+                X[..., -1] = X[..., -1].real.to(torch.complex64)
+        y = _fft.irfft(X * (1.0 / s_fac), n=num, axis=-1)
+    else:
+        if domain == "time":
+            X = _fft.fft(xa.to(torch.complex64), axis=-1)
+        else:
+            X = xa.to(torch.complex64)
+        if W is not None:
+            X = X * _dev(W)
+        first = X[..., :m2]
+        parts = []
+        if num > n:  # upsampling: the unpaired bin is split into a pair
+            if m % 2 == 0:
+                fac = np.ones(m2, dtype=np.float32)
+                fac[-1] = 0.5
+                first = first * _dev(fac)
+                parts = [first]
+                if num - m - 1:
+                    parts.append(torch.zeros(X.shape[:-1] + (num - m - 1,),
+                                             dtype=X.dtype, device=X.device))
+                parts.append(first[..., m2 - 1 : m2])
+            else:
+                parts = [first]
+                if num - m:
+                    parts.append(torch.zeros(X.shape[:-1] + (num - m,), dtype=X.dtype,
+                                             device=X.device))
+        elif num < n:  # downsampling: the bin pair at +-m/2 becomes one unpaired bin
+            if m % 2 == 0:
+                first = torch.cat([first[..., : m2 - 1],
+                                   first[..., m2 - 1 : m2] + X[..., n - m // 2 : n - m // 2 + 1]],
+                                  dim=-1)
+            parts = [first]
+        else:
+            parts = [first]
+        if m2 < m:
+            parts.append(X[..., m2 - m:])
+        Y = parts[0] if len(parts) == 1 else torch.cat(parts, dim=-1)
+        y = _fft.ifft(Y * (1.0 / s_fac), n=num, axis=-1)
+    if moved:
+        y = y.movedim(-1, axis)
+    if t is not None:
+        tt = np.asarray(to_numpy(t), dtype=np.float64)
+        new_t = tt[0] + (tt[1] - tt[0]) * s_fac * np.arange(num)
+        return y, torch.from_numpy(new_t.astype(np.float32)).to(y.device)
+    return y

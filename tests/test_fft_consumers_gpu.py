@@ -1,0 +1,101 @@
+"""GPU parity of the long-FFT consumers against float64 scipy: hilbert, resample (Fourier
+method), fftconvolve, oaconvolve (ports of the reference's filtering / resampling / convolution
+tests). Lengths cover both the three-pass kernels (power-of-two transforms >= 2^12) and the
+composed cuFFT path (other lengths)."""
+
+import numpy as np
+import pytest
+import scipy.signal as sps
+import torch
+
+import mlx_signal_b200 as msig
+from _utils import assert_close
+
+pytestmark = pytest.mark.gpu
+
+
+def peak_err(got, ref):
+    got = got.cpu().numpy() if isinstance(got, torch.Tensor) else np.asarray(got)
+    return float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-30))
+
+
+@pytest.mark.parametrize("n,N", [(1000, None), (1 << 14, None), (1 << 21, None), (5000, 1 << 13),
+                                 (1 << 20, 1 << 21), (777, None)])
+def test_hilbert_matches_scipy(rng, n, N):
+    x = rng.standard_normal((2, n)).astype(np.float32)
+    ref = sps.hilbert(x.astype(np.float64), N=N, axis=-1)
+    got = msig.hilbert(x, N=N)
+    assert got.dtype == torch.complex64 and tuple(got.shape) == ref.shape
+    assert peak_err(got, ref) < 2e-6
+
+
+def test_hilbert_axis_and_errors(rng):
+    x = rng.standard_normal((4096, 3)).astype(np.float32)
+    assert peak_err(msig.hilbert(x, axis=0), sps.hilbert(x.astype(np.float64), axis=0)) < 2e-6
+    with pytest.raises(ValueError):
+        msig.hilbert(x.astype(np.complex64))
+    with pytest.raises(ValueError):
+        msig.hilbert(x, N=0)
+
+
+@pytest.mark.parametrize("n,num", [(1 << 14, 3000), (1 << 14, 1 << 15), (1000, 1500),
+                                   (1001, 600), (1 << 21, 1 << 20), (1 << 20, 1 << 22)])
+@pytest.mark.parametrize("window", [None, "hann"])
+def test_resample_real_matches_scipy(rng, n, num, window):
+    x = rng.standard_normal((2, n)).astype(np.float32)
+    ref = sps.resample(x.astype(np.float64), num, axis=-1, window=window)
+    got = msig.resample(x, num, axis=-1, window=window)
+    assert tuple(got.shape) == ref.shape
+    assert peak_err(got, ref) < 5e-6
+
+
+@pytest.mark.parametrize("n,num", [(4096, 1000), (4096, 9000), (999, 1000), (1000, 999)])
+def test_resample_complex_and_freq_domain(rng, n, num):
+    x = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    ref = sps.resample(x.astype(np.complex128), num)
+    assert peak_err(msig.resample(x, num), ref) < 5e-6
+    X = np.fft.fft(x.astype(np.complex128))
+    ref_f = sps.resample(X, num, domain="freq")
+    assert peak_err(msig.resample(X.astype(np.complex64), num, domain="freq"), ref_f) < 5e-6
+    t = np.linspace(0, 1, n, endpoint=False)
+    _, nt_ref = sps.resample(x.astype(np.complex128), num, t=t)
+    _, nt = msig.resample(x, num, t=t)
+    np.testing.assert_allclose(nt.cpu().numpy(), nt_ref, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("n1,n2", [(1 << 20, 1 << 20), (1 << 21, 4097), (5000, 300), (300, 5000),
+                                   (1 << 15, 1 << 12)])
+@pytest.mark.parametrize("mode", ["full", "same", "valid"])
+def test_fftconvolve_matches_scipy(rng, n1, n2, mode):
+    a = rng.standard_normal(n1).astype(np.float32)
+    b = rng.standard_normal(n2).astype(np.float32)
+    ref = sps.fftconvolve(a.astype(np.float64), b.astype(np.float64), mode=mode)
+    got = msig.fftconvolve(a, b, mode=mode)
+    assert tuple(got.shape) == ref.shape
+    assert peak_err(got, ref) < 5e-6
+
+
+def test_fftconvolve_nd_complex_and_errors(rng):
+    a = rng.standard_normal((3, 2000)).astype(np.float32)
+    b = rng.standard_normal((1, 300)).astype(np.float32)
+    ref = sps.fftconvolve(a.astype(np.float64), b.astype(np.float64), mode="same", axes=-1)
+    assert peak_err(msig.fftconvolve(a, b, mode="same", axes=-1), ref) < 5e-6
+    c = (rng.standard_normal((40, 50)) + 1j * rng.standard_normal((40, 50))).astype(np.complex64)
+    d = rng.standard_normal((7, 9)).astype(np.float32)
+    ref2 = sps.fftconvolve(c.astype(np.complex128), d.astype(np.float64))
+    assert peak_err(msig.fftconvolve(c, d), ref2) < 5e-6
+    with pytest.raises(ValueError):
+        msig.fftconvolve(a, b[0])
+    with pytest.raises(ValueError):
+        msig.fftconvolve(a, b, mode="nope")
+
+
+@pytest.mark.parametrize("n1,n2", [(1 << 20, 513), (100000, 2048), (3000, 3000), (257, 4096)])
+@pytest.mark.parametrize("mode", ["full", "same", "valid"])
+def test_oaconvolve_matches_scipy(rng, n1, n2, mode):
+    a = rng.standard_normal((2, n1)).astype(np.float32)
+    b = rng.standard_normal((2, n2)).astype(np.float32)
+    ref = sps.oaconvolve(a.astype(np.float64), b.astype(np.float64), mode=mode, axes=-1)
+    got = msig.oaconvolve(a, b, mode=mode, axes=-1)
+    assert tuple(got.shape) == ref.shape
+    assert peak_err(got, ref) < 5e-6
