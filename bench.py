@@ -481,7 +481,54 @@ def secondary(x, steps, warmup, dist, clocks):
     del y, z, xr
     out["batched_512_uneven"] = batched_uneven(dist, clocks, peak)
     out["rfft_1x2p23"] = large_rfft(dist, clocks, peak)
+    out["fft_consumers"] = fft_consumers(dist, clocks, peak)
     return out
+
+
+def fft_consumers(dist, clocks, peak, seed=9):
+    """The long-FFT consumers on power-of-two sizes the three-pass kernels take, each against
+    scipy (float64 result, one host call) on the same float32 input."""
+    import torch
+    import scipy.signal as sps
+
+    import mlx_signal_b200 as msig
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    n = 1 << 22
+    x = torch.randn(n, generator=g, device=dev)
+    y = torch.randn(n, generator=g, device=dev)
+    h = torch.randn(1025, generator=g, device=dev)
+    xh, yh, hh = x.cpu().numpy(), y.cpu().numpy(), h.cpu().numpy()
+    cases = {
+        "hilbert_2p23": (lambda: msig.hilbert(torch.cat([x, y])),
+                         lambda: sps.hilbert(np.concatenate([xh, yh])), (1 << 23) * 12),
+        "fftconvolve_2p22_x_2p22": (lambda: msig.fftconvolve(x, y),
+                                    lambda: sps.fftconvolve(xh, yh), 2 * n * 4 + (2 * n - 1) * 4),
+        "oaconvolve_2p22_x_1025": (lambda: msig.oaconvolve(x, h),
+                                   lambda: sps.oaconvolve(xh, hh), n * 4 + 1025 * 4 + (n + 1024) * 4),
+        "resample_2p22_to_3x2p20": (lambda: msig.resample(x, 3 << 20),
+                                    lambda: sps.resample(xh, 3 << 20), n * 4 + (3 << 20) * 4),
+    }
+    res = {}
+    for name, (gpu, cpu, nbytes) in cases.items():
+        got = gpu()
+        ref = cpu()
+        err = float(np.max(np.abs(got.cpu().numpy() - ref)) / np.max(np.abs(ref)))
+        ms = timed(gpu, 10, 2, dist, clocks)
+        t = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            cpu()
+            t.append(time.perf_counter() - t0)
+        cpu_gbs = nbytes / min(t) / 1e9
+        res[name] = {"ms": ms, "GB/s": nbytes / ms / 1e6, "frac_hbm": nbytes / ms / 1e6 / peak,
+                     "max_abs_err_rel_peak_vs_scipy_f64": err,
+                     "cpu_baseline": {"GB/s": cpu_gbs, "cores": 1, "kind": "port",
+                                      "sample": "the full transform, one scipy call"},
+                     "speedup_vs_cpu": nbytes / ms / 1e6 / cpu_gbs}
+    return res
 
 
 def batched_uneven(dist, clocks, peak, nreq=512, seed=11):
