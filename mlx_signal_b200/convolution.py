@@ -6,7 +6,8 @@ sliced to the 'full' / 'same' / 'valid' output. Along a single axis the padded l
 of two when the three-pass kernels (`mlx_signal_b200.fft`) cover it and it costs at most a
 quarter more than the 5-smooth length scipy would use; otherwise, and for several axes, cuFFT runs
 through torch (the composed GPU path). `oaconvolve` cuts the longer input into blocks, transforms
-all blocks as one batch, multiplies by the short input's spectrum and overlap-adds the blocks.
+all blocks as one batch (short transforms: cuFFT), multiplies by the short input's spectrum and
+overlap-adds the blocks.
 Results are float32 (complex64 if either input is complex) on the GPU.
 """
 
@@ -143,9 +144,8 @@ def fftconvolve(in1, in2, mode="full", axes=None):
 
 def _oa_block(n_long: int, n_short: int) -> int:
     """Block length: the transform length F = block + n_short - 1 is the smallest power of two
-    at least 4x the short input (and >= 2^13 so the three-pass kernels take it), capped by the
-    long input."""
-    f = max(1 << 13, 1 << max(0, (4 * n_short - 1).bit_length()))
+    at least 4x the short input (at least 256), capped by the long input."""
+    f = max(1 << 8, 1 << max(0, (4 * n_short - 1).bit_length()))
     return max(1, min(f - n_short + 1, n_long))
 
 

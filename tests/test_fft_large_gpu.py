@@ -13,6 +13,13 @@ from mlx_signal_b200 import fft as bfft
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def kernels_from_2p12(monkeypatch):
+    """These tests exercise the three-pass kernels at every length the C-ABI takes (the public
+    routing sends complex lengths below 2^20 to cuFFT)."""
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
+
+
 def _rel(got, ref):
     got = got.cpu().numpy() if isinstance(got, torch.Tensor) else got
     return float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-30))
@@ -101,3 +108,10 @@ def test_error_word_clear_after_transform(rng):
     assert lib.sp_fft_error_word(ws.data_ptr(), n, 1, ctypes.byref(off)) == 0
     torch.cuda.synchronize()
     assert int(ws[off.value : off.value + 4].view(torch.int32).item()) == 0
+
+
+def test_default_routing_uses_cufft_below_2p20(rng, monkeypatch):
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 20)
+    assert not bfft._pow2_in_range(1 << 19) and bfft._pow2_in_range(1 << 20)
+    x = rng.standard_normal(1 << 14).astype(np.float32)
+    assert _rel(bfft.rfft(x), np.fft.rfft(x.astype(np.float64))) < 5e-6
