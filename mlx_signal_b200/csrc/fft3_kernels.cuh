@@ -136,9 +136,11 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
   using CFG = Fft3Cfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
   constexpr int L = PL::L, E = PL::E, P = PL::P;
-  extern __shared__ unsigned char smraw[];
-  const uintptr_t base = (reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023);
-  float2* tiles = reinterpret_cast<float2*>(base);  // two tiles of L x kTileCols
+  extern __shared__ __align__(16) unsigned char smraw[];
+  // 1024-byte alignment for the swizzle, as an offset into the shared array (so every pointer
+  // below stays in the shared address space: LDS/STS, not generic loads)
+  const uint32_t pad = (1024u - (smem_u32(smraw) & 1023u)) & 1023u;
+  float2* tiles = reinterpret_cast<float2*>(smraw + pad);  // two tiles of L x kTileCols
   float2* xbuf = tiles + 2 * L * kTileCols;
   float2* tw = xbuf + kTileCols * PL::BUF;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + PL::TW);
