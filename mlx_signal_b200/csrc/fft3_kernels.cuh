@@ -109,9 +109,11 @@ struct Fft3Cfg {
   static constexpr int L = PL::L;
   static constexpr int THREADS = kTileCols * PL::P;
   static constexpr int TILE_BYTES = L * kTileCols * 8;
-  // two tiles (1024-byte aligned for the swizzle) | exchange buffers | team twiddles | 2 mbarriers
+  // two tiles (1024-byte aligned for the swizzle) | exchange buffers | team twiddles |
+  // per-tile inter-pass twiddles (L + kTileCols double2) | 2 mbarriers
   static constexpr size_t SMEM = 1024 + 2 * size_t(TILE_BYTES) +
-                                 size_t(kTileCols) * PL::BUF * 8 + size_t(PL::TW) * 8 + 16;
+                                 size_t(kTileCols) * PL::BUF * 8 + size_t(PL::TW) * 8 +
+                                 size_t(L + kTileCols) * 16 + 16;
 };
 
 // One pass of the three-pass FFT. PASS 1: tile rows m3 (L = R3), columns r; PASS 2: rows m2
@@ -143,7 +145,8 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
   float2* tiles = reinterpret_cast<float2*>(smraw + pad);  // two tiles of L x kTileCols
   float2* xbuf = tiles + 2 * L * kTileCols;
   float2* tw = xbuf + kTileCols * PL::BUF;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + PL::TW);
+  double2* ttw = reinterpret_cast<double2*>(tw + PL::TW);  // this tile's inter-pass twiddles
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ttw + L + kTileCols);
   const int R1 = pr.R1, R2 = pr.R2, R3 = pr.R3;
   const int64_t N = pr.N;
   if (threadIdx.x == 0) {
@@ -177,6 +180,30 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
     const uint32_t par = uint32_t(it >> 1) & 1u;
     const int nxt = tl + int(gridDim.x);
     if (threadIdx.x == 0 && nxt < pr.ntiles) issue(nxt, j ^ 1);
+    // This tile's inter-pass twiddles, computed while its copy is in flight (the previous
+    // tile's readers finished at the last barrier; the wait below publishes them). Each is an
+    // independent FP64 sincospi of an exactly reduced integer phase:
+    //   pass 1: W_N^(R1 m2 km3) (times 1/N for the inverse), one per output row km3, rounded
+    //           once to FP32 and shared by every column of the tile;
+    //   pass 2: W_N^(r km2 R3) per row km2 and W_N^(r km3) per column km3, kept in FP64 and
+    //           multiplied per element (rounded once).
+    if constexpr (PASS != 3) {
+      int cg_, slab_, b_;
+      fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg_, &slab_, &b_);
+      if constexpr (PASS == 1) {
+        const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
+        float2* t1 = reinterpret_cast<float2*>(ttw);
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+          const double2 w = w_exact(int64_t(R1) * slab_ * i, N);
+          t1[i] = make_float2(float(w.x * sc), float(w.y * sc));
+        }
+      } else {
+        for (int i = threadIdx.x; i < L + kTileCols; i += blockDim.x) {
+          ttw[i] = i < L ? w_exact(int64_t(slab_) * i * R3, N)
+                         : w_exact(int64_t(slab_) * (cg_ * kTileCols + (i - L)), N);
+        }
+      }
+    }
     const bool ok = __syncthreads_and(mbar_wait(bar + j, par) ? 1 : 0) != 0;
     if (!ok) {
       if (threadIdx.x == 0) {
@@ -206,28 +233,20 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
     team_passes<PL>(v, buf, tw, t, mask);
     // output k = t + e*P of this column
     if constexpr (PASS == 1) {
-      // twiddle W_N^(R1 m2 km3), km3 = t + e P; FP64 anchor + recurrence, rounded once
+      // twiddle W_N^(R1 m2 km3) of output row km3 = t + e P, from the tile table
       const int m2 = slab, r = col0 + c;
-      double2 w = w_exact(int64_t(R1) * m2 * t, N);
-      const double2 d = w_exact(int64_t(R1) * m2 * P, N);
-      const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
+      const float2* t1 = reinterpret_cast<const float2*>(ttw);
       float2* dst = pr.out + int64_t(b) * N + (int64_t(m2) * R1 + r) * R3;
-  #pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const float2 wf = make_float2(float(w.x * sc), float(w.y * sc));
-        dst[t + e * P] = cmul(v[e], wf);
-        w = zmul(w, d);
-      }
+#pragma unroll
+      for (int e = 0; e < E; ++e) dst[t + e * P] = cmul(v[e], t1[t + e * P]);
     } else {
       if constexpr (PASS == 2) {
-        // twiddle W_N^(r (km2 R3 + km3)), km2 = t + e P, km3 = col0 + c
-        const int r = slab, km3 = col0 + c;
-        double2 w = w_exact(int64_t(r) * (int64_t(t) * R3 + km3), N);
-        const double2 d = w_exact(int64_t(r) * R3 * P, N);
-  #pragma unroll
+        // twiddle W_N^(r (km2 R3 + km3)) = W_N^(r km2 R3) W_N^(r km3), km2 = t + e P
+        const double2 wc = ttw[L + c];
+#pragma unroll
         for (int e = 0; e < E; ++e) {
+          const double2 w = zmul(ttw[t + e * P], wc);
           v[e] = cmul(v[e], make_float2(float(w.x), float(w.y)));
-          w = zmul(w, d);
         }
       }
       __syncthreads();  // every team has read its column: the tile can be overwritten
