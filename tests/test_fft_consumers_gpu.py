@@ -9,7 +9,6 @@ import scipy.signal as sps
 import torch
 
 import mlx_signal_b200 as msig
-from _utils import assert_close
 
 pytestmark = pytest.mark.gpu
 

@@ -4,7 +4,6 @@ accuracy bar against float64 scipy, stream chunks reproduce scipy.signal.stft of
 concatenated stream, admission respects the HBM budget, and the open-loop Poisson driver and the
 per-request baseline complete their schedules."""
 
-import numpy as np
 import pytest
 import scipy.signal as sps
 import torch
