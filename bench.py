@@ -482,7 +482,66 @@ def secondary(x, steps, warmup, dist, clocks):
     out["batched_512_uneven"] = batched_uneven(dist, clocks, peak)
     out["rfft_1x2p23"] = large_rfft(dist, clocks, peak)
     out["fft_consumers"] = fft_consumers(dist, clocks, peak)
+    out["reference_published_rows"] = published_rows(dist, clocks)
     return out
+
+
+#: the reference's published device times for this path (Apple M4 Max, MLX 0.32.2, float32;
+#: median of 9 after 3 warm-ups): (label, ms)
+PUBLISHED_ROWS = {
+    "welch_1x2p22_n4096": 0.65,
+    "welch_256x2p16_n256": 0.98,
+    "csd_64x2p20_n1024": 7.68,
+    "coherence_64x2p20_n1024": 8.40,
+    "spectrogram_16x2p20_n1024": 1.31,
+    "stft_16x2p20_n1024": 1.25,
+    "istft_16x2p20_n1024": 1.50,
+}
+
+
+def published_rows(dist, clocks, seed=13):
+    """Our device time on each shape the reference publishes a device time for, through the public
+    API with device-resident float32 input (host argument handling included, as in the
+    reference's 'device' column), and config 1 (1 x 2^16 welch, nperseg 256): public API, and a
+    CUDA-graph replay of the same launch sequence."""
+    import torch
+
+    import mlx_signal_b200 as msig
+    from mlx_signal_b200 import graphs
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    big = torch.randn((64, 1 << 20), generator=g, device=dev)
+    y = torch.randn((64, 1 << 20), generator=g, device=dev)
+    x16 = big[:16]
+    w4096 = torch.randn((1, 1 << 22), generator=g, device=dev)
+    w256 = torch.randn((256, 1 << 16), generator=g, device=dev)
+    _, _, z16 = msig.stft(x16, nperseg=1024)
+    calls = {
+        "welch_1x2p22_n4096": lambda: msig.welch(w4096, nperseg=4096),
+        "welch_256x2p16_n256": lambda: msig.welch(w256, nperseg=256),
+        "csd_64x2p20_n1024": lambda: msig.csd(big, y, nperseg=1024),
+        "coherence_64x2p20_n1024": lambda: msig.coherence(big, y, nperseg=1024),
+        "spectrogram_16x2p20_n1024": lambda: msig.spectrogram(x16, nperseg=1024, noverlap=512,
+                                                              window="hann"),
+        "stft_16x2p20_n1024": lambda: msig.stft(x16, nperseg=1024),
+        "istft_16x2p20_n1024": lambda: msig.istft(z16, nperseg=1024),
+    }
+    res = {}
+    for name, fn in calls.items():
+        ms = timed(fn, 20, 3, dist, clocks)
+        res[name] = {"ms": ms, "reference_device_ms_m4max": PUBLISHED_ROWS[name],
+                     "speedup_vs_reference_published": PUBLISHED_ROWS[name] / ms}
+    # config 1: 1 x 2^16 welch, nperseg 256 (launch-bound)
+    x1 = torch.randn((1, 1 << 16), generator=g, device=dev)
+    ms_api = timed(lambda: msig.welch(x1, nperseg=256), 50, 5, dist, clocks)
+    _, call = graphs.graphed_welch(x1, nperseg=256)
+    ms_graph = timed(lambda: call(x1), 50, 5, dist, clocks)
+    res["config1_welch_1x2p16_n256"] = {"ms_public_api": ms_api, "ms_cuda_graph_replay": ms_graph,
+                                        "alg_bytes": (1 << 16) * 4 + 129 * 4,
+                                        "note": "launch-bound: microseconds, not roofline"}
+    return res
 
 
 def fft_consumers(dist, clocks, peak, seed=9):

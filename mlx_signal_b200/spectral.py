@@ -25,7 +25,7 @@ import torch
 from . import _kernels
 from ._array import device, input_shape, input_size, to_device, to_numpy
 from ._config import composed_path_notice
-from .windows import _window_np, device_vector
+from .windows import DEVICE_CONSTANTS, _window_np, device_vector
 
 __all__ = ["coherence", "csd", "istft", "periodogram", "spectrogram", "stft", "welch"]
 
@@ -134,9 +134,36 @@ def _empty(shape) -> torch.Tensor:
     return torch.zeros(tuple(shape), dtype=torch.float32, device=device())
 
 
+def _axis_vector(key: tuple, build) -> torch.Tensor:
+    """A fresh device copy of a cached float32 axis vector (frequencies, segment times): the
+    host values are uploaded once per key, later calls cost one device-to-device copy instead
+    of a pageable upload that would wait for the stream."""
+    dev = device()
+    k = key + (dev.index,)
+    hit = DEVICE_CONSTANTS.get(k)
+    if hit is None:
+        hit = torch.from_numpy(np.ascontiguousarray(build(), dtype=np.float32)).to(dev)
+        DEVICE_CONSTANTS.put(k, hit, hit.numel() * 4 + 64)
+    return hit.clone()
+
+
 def _freqs(nfft: int, fs: float, onesided: bool) -> torch.Tensor:
-    f = np.fft.rfftfreq(nfft, 1 / fs) if onesided else np.fft.fftfreq(nfft, 1 / fs)
-    return torch.from_numpy(f.astype(np.float32)).to(device())
+    def build():
+        return np.fft.rfftfreq(nfft, 1 / fs) if onesided else np.fft.fftfreq(nfft, 1 / fs)
+
+    return _axis_vector(("freqs", int(nfft), float(fs), bool(onesided)), build)
+
+
+def _times(s) -> torch.Tensor:
+    """Segment centre times (scipy's t vector; boundary-extended inputs start at 0)."""
+    def build():
+        t_np = np.arange(s.nperseg / 2, s.n_total - s.nperseg / 2 + 1, s.nstep) / float(s.fs)
+        if s.boundary is not None:
+            t_np = t_np - (s.nperseg / 2) / s.fs
+        return t_np
+
+    key = ("times", s.nperseg, s.nstep, s.n_total, float(s.fs), s.boundary is not None)
+    return _axis_vector(key, build)
 
 
 def _pad_last(t: torch.Tensor, n: int) -> torch.Tensor:
@@ -272,10 +299,6 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
     s.boundary, s.ext, s.n_orig, s.n_total = boundary, ext, n_orig, n_ext + nadd
     s.win = device_vector((win_np * np.sqrt(scale)).astype(np.float32))
     s.freqs = _freqs(nfft, fs, onesided)
-    t_np = np.arange(nperseg / 2, s.n_total - nperseg / 2 + 1, nstep) / float(fs)
-    if boundary is not None:
-        t_np = t_np - (nperseg / 2) / fs
-    s.t = torch.from_numpy(t_np.astype(np.float32)).to(device())
     s.fused = (not x_complex) and (not y_complex) and _kernels.fused_mean_ok(nfft)
     return s
 
@@ -331,6 +354,55 @@ def _freq_axis_out(result: torch.Tensor, axis: int) -> torch.Tensor:
 # ---------------------------------------------------------------------------------------------
 
 
+class _WelchPlan:
+    """Everything a fused mean-PSD call derives from its arguments and input shape: the scaled
+    device window, the spectral-detrend table, the kernel geometry and the cached frequency
+    vector. A repeated call with the same arguments and shape runs the kernel straight away
+    (input layout handling, the C-ABI call, one copy of the frequency vector)."""
+
+    def __init__(self, s, rows: int, n: int, outer: tuple):
+        self.win, self.wdft = s.win, _spectral_detrend_table(s)
+        self.geom = (s.nperseg, s.nfft, s.nstep, s.code, s.onesided)
+        self.rows, self.n, self.outer, self.axis = rows, n, outer, s.axis
+        self.freqs = s.freqs.clone()
+
+    def run(self, x: torch.Tensor):
+        X = x.movedim(self.axis, -1) if x.dim() > 1 and self.axis != -1 else x
+        res = _kernels.welch_mean(X.reshape(self.rows, self.n), self.win, *self.geom,
+                                  wdft=self.wdft)
+        pxy = res.reshape(self.outer + (res.shape[-1],))
+        if pxy.dim() > 1 and self.axis != -1:
+            pxy = pxy.movedim(-1, self.axis if self.axis >= 0 else pxy.dim() + self.axis)
+        return self.freqs.clone(), pxy
+
+
+_PLANS: dict = {}
+
+
+def _plan_key(x, same, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
+              axis, average):
+    """Hashable key of a welch-type call eligible for the plan cache (CUDA float32 tensor input
+    on the current device, named window), else None."""
+    if not (same and average == "mean" and isinstance(x, torch.Tensor) and x.is_cuda
+            and x.dtype == torch.float32 and isinstance(window, str | tuple)):
+        return None
+    if x.device != device():
+        return None
+    key = (tuple(x.shape), x.device.index, fs, window, nperseg, noverlap, nfft,
+           type(detrend).__name__, detrend, return_onesided, scaling, axis)
+    try:
+        hash(key)
+    except TypeError:
+        return None
+    return key
+
+
+def _remember_plan(key, plan) -> None:
+    if len(_PLANS) >= 256:
+        _PLANS.clear()
+    _PLANS[key] = plan
+
+
 def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
         detrend="constant", return_onesided=True, scaling="density", axis=-1, average="mean"):
     """Cross power spectral density Pxy by Welch's method (scipy.signal.csd semantics).
@@ -341,6 +413,11 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     if average not in ("mean", "median"):
         raise ValueError(f"average must be 'mean' or 'median', got {average!r}")
     same = y is x
+    key = _plan_key(x, same, fs, window, nperseg, noverlap, nfft, detrend, return_onesided,
+                    scaling, axis, average)
+    plan = _PLANS.get(key) if key is not None else None
+    if plan is not None:
+        return plan.run(x)
     if input_size(x) == 0 or (not same and input_size(y) == 0):
         xs = input_shape(x)
         if same:
@@ -372,6 +449,8 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
             res = _kernels.cross_mean("csd", Xb, Yb, s.win, s.nperseg, s.nfft, s.nstep, s.code,
                                       s.onesided, wdft=_spectral_detrend_table(s))
         pxy = res.reshape(outer + (res.shape[-1],))
+        if same and key is not None and (256 if nperseg is None else int(nperseg)) <= n:
+            _remember_plan(key, _WelchPlan(s, rows, n, outer))
     else:
         rows = int(np.prod(outer)) if outer else 1
         if s.fused:
@@ -547,7 +626,7 @@ def spectrogram(x, fs=1.0, window=("tukey", 0.25), nperseg=None, noverlap=None, 
         if mode == "phase":
             ax = s.axis - 1 if s.axis < 0 else s.axis
             sxx = _unwrap(sxx, axis=ax)
-    return s.freqs, s.t, sxx
+    return s.freqs, _times(s), sxx
 
 
 def stft(x, fs=1.0, window="hann", nperseg=256, noverlap=None, nfft=None, detrend=False,
@@ -561,7 +640,7 @@ def stft(x, fs=1.0, window="hann", nperseg=256, noverlap=None, nfft=None, detren
                axis, "stft", boundary, padded, True)
     if s.empty is not None:
         return s.empty
-    return s.freqs, s.t, _freq_axis_out(_frames_result(s, "stft"), s.axis)
+    return s.freqs, _times(s), _freq_axis_out(_frames_result(s, "stft"), s.axis)
 
 
 def _istft_axes(shape, freq_axis: int, time_axis: int):

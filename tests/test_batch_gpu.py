@@ -172,3 +172,16 @@ def test_autotune_records_a_schedule(tmp_path):
     assert g in (8, 32)
     assert cache.get("welch", 1024, 4) == g
     assert set(cache.entries()["welch/1024/float32/c4"]["us"]) == {"8", "32"}
+
+
+def test_graphed_welch_replays_new_data(rng):
+    from mlx_signal_b200 import graphs
+
+    x0 = torch.from_numpy(rng.standard_normal((2, 1 << 16)).astype(np.float32)).cuda()
+    f, call = graphs.graphed_welch(x0, fs=2.0, nperseg=256)
+    for _ in range(3):
+        x = torch.from_numpy(rng.standard_normal((2, 1 << 16)).astype(np.float32)).cuda()
+        p = call(x).clone()
+        f_ref, p_ref = sps.welch(x.double().cpu().numpy(), fs=2.0, nperseg=256)
+        np.testing.assert_allclose(f.cpu().numpy(), f_ref, rtol=1e-6)
+        assert rel_err_bins(p, p_ref) <= TOL

@@ -287,3 +287,34 @@ def test_half_overlap_cross_spectra_match_scipy(rng, nperseg, detrend):
         ct = _kernels.cross_mean("csd", torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(), w,
                                  nperseg, nperseg, nperseg // 2, 1, True)
         assert rel_err_bins(ct, c_ref) <= 1e-5
+
+
+@pytest.mark.parametrize("shape,axis", [((3, 4096), -1), ((4096, 2), 0)])
+def test_welch_plan_cache_repeats(rng, shape, axis):
+    """Repeated calls with one argument set reuse a cached plan: every call still matches scipy,
+    the frequency vector is a fresh tensor each time, and other arguments get their own plan."""
+    for rep in range(3):
+        x = make_sig(rng, shape)
+        f, p = msig.welch(torch.from_numpy(x).cuda(), fs=4.0, nperseg=256, axis=axis)
+        f_ref, p_ref = sps.welch(x.astype(np.float64), fs=4.0, nperseg=256, axis=axis)
+        assert_close(f, f_ref)
+        assert_close(p, p_ref)
+        f.fill_(-1.0)  # the caller owns the returned vector
+    x = make_sig(rng, shape)
+    f, p = msig.welch(torch.from_numpy(x).cuda(), fs=4.0, nperseg=128, axis=axis,
+                      scaling="spectrum")
+    f_ref, p_ref = sps.welch(x.astype(np.float64), fs=4.0, nperseg=128, axis=axis,
+                             scaling="spectrum")
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+
+
+def test_welch_plan_cache_keeps_warnings_and_errors(rng):
+    xt = torch.from_numpy(make_sig(rng, (100,))).cuda()
+    for _ in range(2):
+        with pytest.warns(UserWarning, match="nperseg"):
+            msig.welch(xt)
+    xt = torch.from_numpy(make_sig(rng, (1024,))).cuda()
+    msig.welch(xt, detrend=False, nperseg=128)
+    with pytest.raises(ValueError):
+        msig.welch(xt, detrend=0, nperseg=128)
