@@ -15,6 +15,7 @@ counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing 
 
 from __future__ import annotations
 
+import copy
 import functools
 import math
 import warnings
@@ -219,6 +220,65 @@ class _Setup:
     pass
 
 
+_SETUPS: dict = {}
+
+
+def _setup_key(name, x, *args):
+    """Hashable key of a same-input call whose argument handling may be memoised (CUDA float32
+    tensor on the current device, named window), else None."""
+    if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float32
+            and x.numel() > 0 and x.device == device()):
+        return None
+    key = (name, tuple(x.shape), x.device.index) + tuple(
+        (type(a).__name__, a) for a in args)
+    try:
+        hash(key)
+    except TypeError:
+        return None
+    return key
+
+
+def _setup_hit(key, x):
+    """A memoised setup re-bound to input x, or None."""
+    hit = _SETUPS.get(key) if key is not None else None
+    if hit is None:
+        return None
+    s = copy.copy(hit)
+    X = x.movedim(s.axis, -1) if x.dim() > 1 and s.axis != -1 else x
+    s.X = s.Y = X
+    s.freqs = hit.freqs.clone()
+    return s
+
+
+def _remember_setup(key, s) -> None:
+    """Memoise a fused same-input setup (without its input; tables looked up once)."""
+    snap = copy.copy(s)
+    snap.X = snap.Y = None
+    snap.freqs = s.freqs.clone()
+    _spectral_detrend_table(snap, frames=True)
+    _spectral_detrend_table(snap)
+    if len(_SETUPS) >= 256:
+        _SETUPS.clear()
+    _SETUPS[key] = snap
+
+
+def _setup_same(key, x, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
+                axis, mode, boundary, padded):
+    """_setup(x, x, ...) memoised per key: a repeat call with the same input shape and arguments
+    reuses the window, tables and geometry and only re-binds the input (and copies the cached
+    frequency vector). Calls that warn (nperseg longer than the input) are not memoised."""
+    s = _setup_hit(key, x)
+    if s is not None:
+        return s
+    s = _setup(x, x, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
+               axis, mode, boundary, padded, True)
+    requested = 256 if nperseg is None else int(nperseg)
+    if (key is not None and s.empty is None and s.fused and isinstance(window, str | tuple)
+            and requested <= s.n_orig):
+        _remember_setup(key, s)
+    return s
+
+
 def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling, axis,
            mode, boundary, padded, same):
     if mode not in ("psd", "stft"):
@@ -309,10 +369,18 @@ _WDFT_CACHE: dict = {}
 def _spectral_detrend_table(s, frames: bool = False):
     """Low-bin window spectrum (device complex64) enabling the constant detrend as a spectral
     correction in the fused welch kernel (50% overlap, nperseg == nfft) or, with frames=True, in
-    the per-frame kernels (any overlap and nfft); None -> time-domain detrend."""
+    the per-frame kernels (any overlap and nfft); None -> time-domain detrend. Kept on the setup
+    object once looked up."""
+    attr = "wdft_frames" if frames else "wdft_mean"
+    hit = s.__dict__.get(attr, False)
+    if hit is not False:
+        return hit
     if s.code != 1 or (not frames and (s.nperseg != s.nfft or 2 * s.nstep != s.nperseg)):
-        return None
-    return _window_table((s.win_np * np.sqrt(s.scale)).astype(np.float32), s.nfft)
+        val = None
+    else:
+        val = _window_table((s.win_np * np.sqrt(s.scale)).astype(np.float32), s.nfft)
+    s.__dict__[attr] = val
+    return val
 
 
 def _window_table(w32: np.ndarray, nfft: int):
@@ -609,13 +677,21 @@ def spectrogram(x, fs=1.0, window=("tukey", 0.25), nperseg=None, noverlap=None, 
     modelist = ["psd", "complex", "magnitude", "angle", "phase"]
     if mode not in modelist:
         raise ValueError(f"unknown value for mode {mode}, must be one of {modelist}")
-    X = to_device(x)
-    window, nperseg = _triage_segments(window, nperseg, input_length=X.shape[axis])
-    if noverlap is None:
-        noverlap = nperseg // 8
     helper_mode = "psd" if mode == "psd" else "stft"
-    s = _setup(X, X, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
-               axis, helper_mode, None, False, True)
+    key = _setup_key("spectrogram", x, fs, window, nperseg, noverlap, nfft, detrend,
+                     return_onesided, scaling, axis, helper_mode)
+    s = _setup_hit(key, x)
+    if s is None:
+        X = to_device(x)
+        req = nperseg
+        window, nperseg = _triage_segments(window, nperseg, input_length=X.shape[axis])
+        if noverlap is None:
+            noverlap = nperseg // 8
+        s = _setup(X, X, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
+                   axis, helper_mode, None, False, True)
+        if (key is not None and s.empty is None and s.fused
+                and (256 if req is None else int(req)) <= s.n_orig):
+            _remember_setup(key, s)
     if s.empty is not None:
         return s.empty
     sxx = _freq_axis_out(_frames_result(s, helper_mode), s.axis)
@@ -636,8 +712,10 @@ def stft(x, fs=1.0, window="hann", nperseg=256, noverlap=None, nfft=None, detren
         scaling = "density"
     elif scaling != "spectrum":
         raise ValueError(f"Parameter {scaling=} not in ['spectrum', 'psd']!")
-    s = _setup(x, x, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
-               axis, "stft", boundary, padded, True)
+    key = _setup_key("stft", x, fs, window, nperseg, noverlap, nfft, detrend, return_onesided,
+                     boundary, padded, axis, scaling)
+    s = _setup_same(key, x, fs, window, nperseg, noverlap, nfft, detrend, return_onesided,
+                    scaling, axis, "stft", boundary, padded)
     if s.empty is not None:
         return s.empty
     return s.freqs, _times(s), _freq_axis_out(_frames_result(s, "stft"), s.axis)
@@ -661,6 +739,36 @@ def _istft_axes(shape, freq_axis: int, time_axis: int):
 
 
 _NOLA_CACHE: dict = {}
+_ISTFT_PLANS: dict = {}
+
+
+class _IstftPlan:
+    """Fused-path istft for one input shape and argument set: device window, scale, geometry,
+    the NOLA verdict and the output time vector, derived once."""
+
+    def __init__(self, win, scale, nperseg, nstep, batch, outputlength, boundary, nola_ok, perm,
+                 fs, freq_ax, time_ax):
+        self.win, self.scale, self.nperseg, self.nstep = win, scale, nperseg, nstep
+        self.batch, self.outputlength, self.boundary = batch, outputlength, boundary
+        self.nola_ok, self.perm, self.fs = nola_ok, perm, fs
+        self.freq_ax, self.time_ax = freq_ax, time_ax
+        self.rows = int(np.prod(batch)) if batch else 1
+
+    def run(self, Z: torch.Tensor, permuted: bool = False):
+        if not permuted and self.perm != list(range(Z.dim())):
+            Z = Z.permute(self.perm)
+        x = _kernels.istft_fused(Z.reshape((self.rows,) + Z.shape[-2:]), self.win, self.scale,
+                                 self.nperseg, self.nstep)
+        x = x.reshape(self.batch + (self.outputlength,))
+        if self.boundary:
+            x = x[..., self.nperseg // 2 : -(self.nperseg // 2)]
+        if not self.nola_ok:
+            warnings.warn(
+                "NOLA condition failed, STFT may not be invertible."
+                + (" Possibly due to missing boundary" if not self.boundary else ""),
+                stacklevel=3,
+            )
+        return _istft_finish(x, self.fs, self.freq_ax, self.time_ax)
 
 
 def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
@@ -670,6 +778,18 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     Deviation (as in the reference, spectral.py:837-841): for N-d input the returned time
     vector has the length of the output time axis.
     """
+    key = None
+    if (isinstance(Zxx, torch.Tensor) and Zxx.is_cuda and Zxx.dtype == torch.complex64
+            and Zxx.device == device() and isinstance(window, str | tuple)):
+        key = ("istft", tuple(Zxx.shape), Zxx.device.index) + tuple(
+            (type(a).__name__, a) for a in (fs, window, nperseg, noverlap, nfft, input_onesided,
+                                             boundary, time_axis, freq_axis, scaling))
+        try:
+            plan = _ISTFT_PLANS.get(key)
+        except TypeError:
+            key = plan = None
+        if plan is not None:
+            return plan.run(Zxx)
     freq_axis = int(freq_axis)
     time_axis = int(time_axis)
     shape = input_shape(Zxx)
@@ -725,19 +845,15 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     batch = Z.shape[:-2]
     if input_onesided and nfft == nperseg and _kernels.is_pow2(nperseg) and \
             2 <= nperseg <= _kernels.MAX_FUSED_NFFT:
-        rows = int(np.prod(batch)) if batch else 1
-        win = device_vector(win_np.astype(np.float32))
-        x = _kernels.istft_fused(Z.reshape((rows,) + Z.shape[-2:]), win, scale, nperseg, nstep)
-        x = x.reshape(batch + (outputlength,))
-        if boundary:
-            x = x[..., nperseg // 2 : -(nperseg // 2)]
-        if not _nola_ok(win_np, nperseg, nstep, nseg, outputlength, bool(boundary)):
-            warnings.warn(
-                "NOLA condition failed, STFT may not be invertible."
-                + (" Possibly due to missing boundary" if not boundary else ""),
-                stacklevel=2,
-            )
-        return _istft_finish(x, fs, freq_ax, time_ax)
+        plan = _IstftPlan(device_vector(win_np.astype(np.float32)), scale, nperseg, nstep,
+                          batch, outputlength, bool(boundary),
+                          _nola_ok(win_np, nperseg, nstep, nseg, outputlength, bool(boundary)),
+                          perm, fs, freq_ax, time_ax)
+        if key is not None:
+            if len(_ISTFT_PLANS) >= 256:
+                _ISTFT_PLANS.clear()
+            _ISTFT_PLANS[key] = plan
+        return plan.run(Z, permuted=True)
     composed_path_notice("istft", "composed inverse path")
     if input_onesided:
         xsubs = torch.fft.irfft(Z, n=nfft, dim=-1)[..., :nperseg]
@@ -784,7 +900,7 @@ def _istft_finish(x, fs, freq_ax, time_ax):
     out_time_axis = time_ax - (1 if freq_ax < time_ax else 0)
     if x.dim() > 1 and out_time_axis != x.dim() - 1:
         x = x.movedim(-1, out_time_axis)
-    time = torch.arange(n_out, dtype=torch.float32, device=x.device) / float(fs)
+    time = _axis_vector(("istft_time", n_out, float(fs)), lambda: np.arange(n_out) / float(fs))
     return time, x
 
 

@@ -290,3 +290,41 @@ def test_spectral_detrend_frames_match_scipy(rng, nperseg, noverlap, mode):
     # both detrend forms carry an error ~ eps * |mean| * |DFT(w)_0| on the lowest bins (the
     # spectral one from cancellation in the DC bin, the time-domain one from the rounded mean)
     assert float((a - b).abs().max()) <= 1e-5 * float(b.abs().max())
+
+
+@pytest.mark.parametrize("fn", ["stft", "spectrogram"])
+def test_memoised_setup_repeats(rng, fn):
+    """Repeat calls with one argument set reuse the memoised setup: each call matches scipy on its
+    own data; the returned axis vectors belong to the caller; nperseg > n keeps warning."""
+    kw = {"nperseg": 128, "fs": 8.0, "axis": 0}
+    for _ in range(3):
+        x = make_sig(rng, (700, 3))
+        out = getattr(msig, fn)(torch.from_numpy(x).cuda(), **kw)
+        ref = getattr(sps, fn)(x.astype(np.float64), **kw)
+        for a, b in zip(out, ref):
+            assert_close(a, b)
+        out[0].fill_(-1.0)
+        out[1].fill_(-1.0)
+    xs = torch.from_numpy(make_sig(rng, (100,))).cuda()
+    for _ in range(2):
+        with pytest.warns(UserWarning, match="nperseg"):
+            getattr(msig, fn)(xs, nperseg=256)
+
+
+def test_istft_plan_repeats_and_warns(rng):
+    for _ in range(3):
+        x = make_sig(rng, (2, 5000))
+        _, _, z = sps.stft(x.astype(np.float64), nperseg=256)
+        zt = torch.from_numpy(z.astype(np.complex64)).cuda()
+        t, xr = msig.istft(zt, nperseg=256)
+        _, x_ref = sps.istft(z, nperseg=256)
+        # N-d input: the time vector follows the output time axis (as in the reference)
+        assert_close(t, np.arange(x_ref.shape[-1], dtype=np.float64))
+        assert_close(xr, x_ref)
+        t.fill_(-1.0)
+    # boxcar with no overlap and no boundary padding gaps -> NOLA fails on every call
+    z = torch.from_numpy(sps.stft(make_sig(rng, (4096,)), window=("tukey", 0.0), nperseg=256,
+                                  noverlap=0)[2].astype(np.complex64)).cuda()
+    for _ in range(2):
+        with pytest.warns(UserWarning, match="NOLA"):
+            msig.istft(z, window=("tukey", 0.9), nperseg=256, noverlap=0)
