@@ -238,6 +238,23 @@ SP_API int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int ba
  * a tile copy wait gave up); read it after synchronising the stream. */
 SP_API int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_t* offset);
 
+/*
+ * FFT convolution of each of `rows` real rows x (n1 samples, row stride ld_x) with one real filter
+ * h of n2 <= 2049 taps: out[r * ld_out + i] = (x_r * h)[j0 + i] for i in [0, nout), where
+ * (x_r * h)[j] = sum_k h[k] x_r[j - k] is the full linear convolution (length n1 + n2 - 1;
+ * j0 = 0 gives 'full', the centred windows 'same' / 'valid'). One fused overlap-save kernel:
+ * blocks of L = sp_conv_block_len(n2) samples, two blocks per complex FFT, spectrum multiply and
+ * inverse in registers; no workspace. Replaces the fused block convolution and gather overlap-add
+ * of oaconvolve (_stft_metal.fftconv_blocks, _stft_metal.py:1024-1058 with kernels :900-1003;
+ * _ola_metal.ola_gather, _ola_metal.py:63-78; routed from convolution.py:288-306).
+ */
+SP_API int sp_conv_ols_f32(const float* x, int64_t rows, int64_t n1, int64_t ld_x, const float* h,
+                           int n2, int64_t j0, int64_t nout, float* out, int64_t ld_out,
+                           void* stream);
+
+/* Block length the convolution uses for n2 taps, or SP_ERR_UNSUPPORTED when n2 > 2049. */
+SP_API int sp_conv_block_len(int n2);
+
 /* ------------------------------------------------------------------------------------------
  * Batched persistent launch: many welch requests and streaming-STFT chunks of uneven size and
  * nperseg in one kernel launch over a device work queue. The reference has no batched form; a

@@ -227,3 +227,26 @@ def istft_fused(z: torch.Tensor, win: torch.Tensor, scale: float, nperseg: int, 
         "sp_istft_f32",
     )
     return out
+
+
+#: longest filter the fused overlap-save convolution takes
+CONV_MAX_TAPS = 2049
+
+
+def conv_ols(x: torch.Tensor, h: torch.Tensor, j0: int, nout: int) -> torch.Tensor:
+    """Full linear convolution window [j0, j0 + nout) of every row of x (rows, n1) float32 CUDA
+    with one real filter h (n2 <= CONV_MAX_TAPS taps) -> (rows, nout) float32, in one fused
+    overlap-save kernel."""
+    x, ld = _rows(x)
+    rows, n1 = x.shape
+    h = h.reshape(-1)
+    assert h.is_cuda and h.dtype == torch.float32
+    h = h.contiguous()
+    out = torch.empty((rows, nout), dtype=torch.float32, device=x.device)
+    _lib.check(
+        _lib.load().sp_conv_ols_f32(x.data_ptr(), rows, n1, ld, h.data_ptr(), h.numel(), int(j0),
+                                    int(nout), out.data_ptr(), max(int(nout), 1),
+                                    stream_handle()),
+        "sp_conv_ols_f32",
+    )
+    return out

@@ -8,6 +8,10 @@ quarter more than the 5-smooth length scipy would use; otherwise, and for severa
 through torch (the composed GPU path). `oaconvolve` cuts the longer input into blocks, transforms
 all blocks as one batch (short transforms: cuFFT), multiplies by the short input's spectrum and
 overlap-adds the blocks.
+Real data convolved with one filter of at most 2049 taps along one axis (the reference's fused
+block-convolution case, convolution.py:288-306) runs the fused overlap-save kernel
+(`sp_conv_ols_f32`) in both functions: one launch, blocks of up to 4096 samples, the mode's
+output window written directly.
 Results are float32 (complex64 if either input is complex) on the GPU.
 """
 
@@ -18,6 +22,7 @@ import math
 import numpy as np
 import torch
 
+from . import _kernels
 from . import fft as _fft
 from ._array import to_device
 
@@ -123,8 +128,37 @@ def _freq_conv(a1, a2, axes, shape, same_input=False):
     return ret[idx]
 
 
+def _fused_ols(a1, a2, axes, s1, s2, mode):
+    """The fused overlap-save kernel's result when it covers the call (one real convolution
+    axis, the shorter input a single filter of at most CONV_MAX_TAPS taps: size 1 on every other
+    axis), else None. The kernel writes the mode's window of the full convolution directly."""
+    if len(axes) != 1 or a1.is_complex() or a2.is_complex():
+        return None
+    ax = axes[0]
+    longer, shorter = (a1, a2) if s1[ax] >= s2[ax] else (a2, a1)
+    if shorter.shape[ax] > _kernels.CONV_MAX_TAPS or any(
+            d != 1 for i, d in enumerate(shorter.shape) if i != ax):
+        return None
+    n1, n2 = longer.shape[ax], shorter.shape[ax]
+    full = n1 + n2 - 1
+    if mode == "full":
+        j0, nout = 0, full
+    else:
+        nout = s1[ax] if mode == "same" else s1[ax] - s2[ax] + 1
+        j0 = (full - nout) // 2
+    xl = longer.movedim(ax, -1)
+    lead = tuple(xl.shape[:-1])
+    out = _kernels.conv_ols(xl.reshape(-1, n1), shorter.reshape(-1), j0, nout)
+    out = out.reshape(lead + (nout,)).movedim(-1, ax)
+    if mode == "same":  # scipy centres every axis on in1's shape
+        out = _centered(out, [s1[i] if i != ax else nout for i in range(out.dim())])
+    return out
+
+
 def fftconvolve(in1, in2, mode="full", axes=None):
-    """Convolve two N-dimensional arrays with zero-padded FFTs (scipy semantics)."""
+    """Convolve two N-dimensional arrays with zero-padded FFTs (scipy semantics). A single
+    filter of at most 2049 taps along one axis of real data runs the fused overlap-save kernel
+    (same result; shorter transforms)."""
     a1, a2 = to_device(in1), to_device(in2)
     if a1.dim() == 0 and a2.dim() == 0:
         return a1 * a2
@@ -137,6 +171,9 @@ def fftconvolve(in1, in2, mode="full", axes=None):
     s1, s2 = tuple(a1.shape), tuple(a2.shape)
     if not axes:
         return a1 * a2
+    fused = _fused_ols(a1, a2, axes, s1, s2, mode)
+    if fused is not None:
+        return fused
     shape = [max(s1[i], s2[i]) if i not in axes else s1[i] + s2[i] - 1 for i in range(a1.dim())]
     ret = _freq_conv(a1, a2, axes, shape, same_input=same_input)
     return _apply_mode(ret, s1, s2, mode, axes)
@@ -167,6 +204,9 @@ def oaconvolve(in1, in2, mode="full", axes=None):
     s1, s2 = tuple(a1.shape), tuple(a2.shape)
     if not axes:
         return a1 * a2
+    fused = _fused_ols(a1, a2, axes, s1, s2, mode)
+    if fused is not None:
+        return fused
     shape = [max(s1[i], s2[i]) if i not in axes else s1[i] + s2[i] - 1 for i in range(a1.dim())]
     if len(axes) != 1 or s1[axes[0]] == s2[axes[0]]:
         return _apply_mode(_freq_conv(a1, a2, axes, shape), s1, s2, mode, axes)

@@ -98,3 +98,63 @@ def test_oaconvolve_matches_scipy(rng, n1, n2, mode):
     got = msig.oaconvolve(a, b, mode=mode, axes=-1)
     assert tuple(got.shape) == ref.shape
     assert peak_err(got, ref) < 5e-6
+
+
+# fused overlap-save convolution: real rows, one shared filter of <= 2049 taps
+@pytest.mark.parametrize("n1,n2", [(1 << 20, 1025), (100000, 1), (100000, 2), (70001, 64),
+                                   (5000, 255), (5000, 256), (4099, 2049), (3000, 2049),
+                                   (1, 1), (17, 5), (300, 1500)])
+@pytest.mark.parametrize("mode", ["full", "same", "valid"])
+@pytest.mark.parametrize("fn", ["fftconvolve", "oaconvolve"])
+def test_fused_conv_matches_scipy(rng, n1, n2, mode, fn):
+    a = rng.standard_normal((3, n1)).astype(np.float32)
+    b = rng.standard_normal((1, n2)).astype(np.float32)
+    if mode == "valid" and n1 < n2:
+        a, b = a[:1], np.broadcast_to(b, (1, n2))
+    ref = getattr(sps, fn)(a.astype(np.float64), b.astype(np.float64), mode=mode, axes=-1)
+    got = getattr(msig, fn)(a, b, mode=mode, axes=-1)
+    assert got.dtype == torch.float32 and tuple(got.shape) == ref.shape
+    assert peak_err(got, ref) < 2e-6
+
+
+def test_fused_conv_axis_swap_and_batch_edges(rng):
+    # filter first (convolution commutes), non-last axis, torch CUDA input, 1-D
+    x = rng.standard_normal((20000, 2)).astype(np.float32)
+    h = rng.standard_normal((33, 1)).astype(np.float32)
+    for mode in ("full", "same", "valid"):
+        ref = sps.oaconvolve(x.astype(np.float64), h.astype(np.float64), mode=mode, axes=0)
+        got = msig.oaconvolve(torch.from_numpy(x).cuda(), h, mode=mode, axes=0)
+        assert tuple(got.shape) == ref.shape and peak_err(got, ref) < 2e-6
+        ref = sps.fftconvolve(h.astype(np.float64), x.astype(np.float64), mode=mode, axes=0)
+        got = msig.fftconvolve(h, x, mode=mode, axes=0)
+        assert tuple(got.shape) == ref.shape and peak_err(got, ref) < 2e-6
+    # 'same' centres on in1's shape on every axis, the batch axis included
+    a = rng.standard_normal((1, 900)).astype(np.float32)
+    b = rng.standard_normal((4, 50)).astype(np.float32)
+    for fn in ("fftconvolve", "oaconvolve"):
+        ref = getattr(sps, fn)(b.astype(np.float64), a.astype(np.float64), mode="same", axes=-1)
+        got = getattr(msig, fn)(b, a, mode="same", axes=-1)
+        assert tuple(got.shape) == ref.shape and peak_err(got, ref) < 2e-6
+    a1 = rng.standard_normal(12345).astype(np.float32)
+    h1 = rng.standard_normal(700).astype(np.float32)
+    assert peak_err(msig.fftconvolve(a1, h1), np.convolve(a1.astype(np.float64), h1)) < 2e-6
+
+
+def test_conv_ols_capi_windows(rng):
+    """The C-ABI entry point writes exactly the requested window of the full convolution into a
+    strided output, leaving the row padding untouched."""
+    from mlx_signal_b200 import _lib
+    from mlx_signal_b200._array import stream_handle
+
+    lib = _lib.load()
+    x = rng.standard_normal((2, 9000)).astype(np.float32)
+    h = rng.standard_normal(129).astype(np.float32)
+    full = np.stack([np.convolve(r.astype(np.float64), h) for r in x])
+    xd, hd = torch.from_numpy(x).cuda(), torch.from_numpy(h).cuda()
+    for j0, nout in [(0, 9128), (5, 100), (128, 8872), (9127, 1), (3000, 4000)]:
+        out = torch.full((2, nout + 7), 7.0, device="cuda")
+        _lib.check(lib.sp_conv_ols_f32(xd.data_ptr(), 2, 9000, 9000, hd.data_ptr(), 129, j0, nout,
+                                       out.data_ptr(), nout + 7, stream_handle()), "conv")
+        o = out.cpu().numpy()
+        assert peak_err(torch.from_numpy(o[:, :nout]), full[:, j0 : j0 + nout]) < 2e-6
+        assert np.all(o[:, nout:] == 7.0)

@@ -89,3 +89,26 @@ def test_window_cache_and_byte_budget():
     assert c.get(("a",)) is None and c.get(("b",)) == 2
     c.put(("huge",), 3, 1000)
     assert c.get(("huge",)) is None
+
+
+def test_conv_ols_block_choice_and_argument_errors():
+    """Host side of the fused convolution entry point: block length per filter length (fewest FFT
+    operations per output with a step of at least half a block) and argument checks, which run
+    before any device work."""
+    from mlx_signal_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.sp_conv_block_len(1) == 256
+    assert lib.sp_conv_block_len(129) == 1024  # 10*1024/896 < 9*512/384 < 8*256/128
+    assert lib.sp_conv_block_len(1025) == 4096
+    assert lib.sp_conv_block_len(2049) == 4096
+    assert lib.sp_conv_block_len(2050) == _lib.SP_ERR_UNSUPPORTED
+    assert lib.sp_conv_block_len(0) == _lib.SP_ERR_UNSUPPORTED
+    dummy = 16  # never dereferenced: the checks below fail before any launch
+    assert lib.sp_conv_ols_f32(dummy, 1, 100, 100, dummy, 10, 0, 110, dummy, 110, None) == \
+        _lib.SP_ERR_ARG  # window past the full length 109
+    assert lib.sp_conv_ols_f32(dummy, 1, 100, 99, dummy, 10, 0, 10, dummy, 10, None) == \
+        _lib.SP_ERR_ARG  # row stride below n1
+    assert lib.sp_conv_ols_f32(dummy, 1, 4000, 4000, dummy, 2050, 0, 10, dummy, 10, None) == \
+        _lib.SP_ERR_UNSUPPORTED
+    assert lib.sp_conv_ols_f32(dummy, 0, 100, 100, dummy, 10, 0, 109, dummy, 109, None) == _lib.SP_OK
