@@ -12,12 +12,21 @@ constexpr int kMaxLog = kMaxLogL;
 
 }  // namespace
 
-__global__ void k_reduce_mean(ReduceParams p) {
+// One CTA of kRedGroups warps per (row, 32 consecutive output bins): warp g sums the row's
+// partial slots c = g, g + kRedGroups, ... in FP64 for its 32 bins (loads coalesced over the
+// bins), then warp 0 adds the group sums in group order. The order is fixed by the launch
+// geometry alone, so results are deterministic; a row spread over hundreds of teams (few rows)
+// is summed by kRedGroups warps per bin instead of one thread.
+constexpr int kRedGroups = 8;
+
+__global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p) {
   pdl_wait();  // launched as a programmatic dependent of the segment kernel
-  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= p.rows * p.nout) return;
-  const int64_t r = idx / p.nout;
-  const int k = int(idx - r * p.nout);
+  __shared__ double4 red[kRedGroups][32];
+  const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
+  const int64_t chunks = (p.nout + 31) / 32;
+  const int64_t r = blockIdx.x / chunks;
+  const int k = int(blockIdx.x - r * chunks) * 32 + lane;
+  const bool live = k < p.nout;
   const int L = p.L;
   const int kk = (L - k) & (L - 1);
   const int kc = k <= kk ? k : kk;
@@ -25,32 +34,47 @@ __global__ void k_reduce_mean(ReduceParams p) {
   int64_t t1 = last_team(r, p.nseg, p.G);
   if (t1 > p.nteams - 1) t1 = p.nteams - 1;
   const int nsl = int(t1 - t0 + 1);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  if (live) {
+    if (p.mode == 0) {
+      const int stride = welch_slot_floats(L);
+      const float* q = p.partial + r * p.cmax * int64_t(stride) + kc;
+#pragma unroll 4
+      for (int c = grp; c < nsl; c += kRedGroups) a0 += double(q[int64_t(c) * stride]);
+    } else {
+      const int stride = cross_slot_floats(L);
+      const int cq = cross_q_floats(L);
+      const float* base = p.partial + r * p.cmax * int64_t(stride);
+#pragma unroll 2
+      for (int c = grp; c < nsl; c += kRedGroups) {
+        const float* q = base + int64_t(c) * stride;
+        a0 += double(q[k]);
+        a1 += double(q[kk]);
+        a2 += double(q[cq + 2 * kc]);
+        a3 += double(q[cq + 2 * kc + 1]);
+      }
+    }
+  }
+  red[grp][lane] = make_double4(a0, a1, a2, a3);
+  __syncthreads();
+  if (grp != 0 || !live) return;
+  a0 = a1 = a2 = a3 = 0.0;
+#pragma unroll
+  for (int g = 0; g < kRedGroups; ++g) {
+    const double4 v = red[g][lane];
+    a0 += v.x;
+    a1 += v.y;
+    a2 += v.z;
+    a3 += v.w;
+  }
+  const int64_t idx = r * p.nout + k;
   double fac = 1.0 / double(p.nseg);
   if (p.onesided && k != 0 && 2 * k != L) fac *= 2.0;
   if (p.mode == 0) {
-    const int stride = welch_slot_floats(L);
-    const float* q = p.partial + r * p.cmax * int64_t(stride) + kc;
-    double s0 = 0.0, s1 = 0.0;
-    int c = 0;
-    for (; c + 1 < nsl; c += 2) {
-      s0 += double(q[int64_t(c) * stride]);
-      s1 += double(q[int64_t(c + 1) * stride]);
-    }
-    if (c < nsl) s0 += double(q[int64_t(c) * stride]);
-    p.out[idx] = float(0.5 * (s0 + s1) * fac);
+    p.out[idx] = float(0.5 * a0 * fac);
     return;
   }
-  const int stride = cross_slot_floats(L);
-  const int cq = cross_q_floats(L);
-  const float* base = p.partial + r * p.cmax * int64_t(stride);
-  double qk = 0.0, qm = 0.0, cr = 0.0, ci = 0.0;
-  for (int c = 0; c < nsl; ++c) {
-    const float* q = base + int64_t(c) * stride;
-    qk += double(q[k]);
-    qm += double(q[kk]);
-    cr += double(q[cq + 2 * kc]);
-    ci += double(q[cq + 2 * kc + 1]);
-  }
+  const double qk = a0, qm = a1, cr = a2, ci = a3;
   const double pxy_re = 0.5 * ci, pxy_im = 0.25 * (qm - qk);
   if (p.mode == 1) {
     p.out[2 * idx] = float(pxy_re * fac);
@@ -197,11 +221,9 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   rp.nteams = pl.nteams;
   rp.mode = mode;
   rp.out = out;
-  const int64_t nthr = rows * rp.nout;
-  const int tb = 128;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(unsigned(cdiv(nthr, tb)));
-  cfg.blockDim = dim3(tb);
+  cfg.gridDim = dim3(unsigned(rows * cdiv(rp.nout, 32)));
+  cfg.blockDim = dim3(32 * kRedGroups);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];

@@ -196,19 +196,37 @@ struct Plan {
   // output bin held in register e after the last pass (radix E, span P): k = t + e*P
 };
 
-// Fill the twiddle tables of a plan (all passes) into shared memory: FP64 sincospi, rounded once.
+// Master table W_4096^j, j in [0, 4096): every inter-pass twiddle of a plan with L <= 4096 is one
+// of its entries (W_N^m = W_4096^(m 4096/N)). Evaluated at compile time by the same FP64 series
+// as the register constants and rounded to FP32 once, so a CTA fills its tables with a gather
+// from L2 instead of evaluating FP64 sines per entry.
+constexpr int kTwMasterLog = 12;
+constexpr int kTwMasterN = 1 << kTwMasterLog;
+struct TwMaster {
+  float2 v[kTwMasterN];
+};
+constexpr TwMaster make_tw_master() {
+  TwMaster t{};
+  for (int j = 0; j < kTwMasterN; ++j) {
+    const CS w = twiddle(j, kTwMasterN);
+    t.v[j] = float2{float(w.c), float(w.s)};
+  }
+  return t;
+}
+static __device__ const TwMaster g_tw_master = make_tw_master();
+
+// Fill the twiddle tables of a plan (all passes) into shared memory from the master table.
 template <class PL>
 __device__ void build_twiddles(float2* tw, int tid, int nthreads) {
+  static_assert(PL::L <= kTwMasterN, "plan longer than the master twiddle table");
   static_for<1, PL::NPASS>([&](auto pc) {
     constexpr int p = decltype(pc)::value;
     constexpr int R = PL::radix(p), S = PL::span(p), SR = S * R;
+    constexpr int step = kTwMasterN / SR;
     float2* t = tw + PL::tw_off(p);
     for (int e = tid; e < R * S; e += nthreads) {
       const int q = e / S, k = e - q * S;
-      const int m = (k * q) % SR;
-      double s, c;
-      sincospi(-2.0 * double(m) / double(SR), &s, &c);
-      t[e] = make_float2(float(c), float(s));
+      t[e] = g_tw_master.v[((k * q) & (SR - 1)) * step];
     }
   });
 }
