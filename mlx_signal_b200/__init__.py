@@ -19,6 +19,7 @@ from .convolution import fftconvolve, oaconvolve
 from .filtering import hilbert
 from .resampling import resample
 from .spectral import coherence, csd, istft, periodogram, spectrogram, stft, welch
+from .streaming import StreamingSTFT, StreamingWelch
 from .windows import get_window
 
 __version__ = "0.1.0"
@@ -26,6 +27,8 @@ __version__ = "0.1.0"
 __all__ = [
     "Config",
     "DowncastWarning",
+    "StreamingSTFT",
+    "StreamingWelch",
     "FallbackWarning",
     "coherence",
     "config_context",
