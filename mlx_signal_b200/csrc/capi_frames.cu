@@ -43,7 +43,16 @@ int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n
   // confined to bins a team thread holds in its first and last register
   const bool spectral = kind != kFrameCross && detrend == kDetrendConstant && wdft != nullptr &&
                         n_low >= 1 && n_low <= ((1 << log_l) >> team_log_e_rt(log_l));
-  const FrameInfo f = lookup(kind, log_l, detrend, spectral);
+  FrameInfo f = lookup(kind, log_l, detrend, spectral);
+  // 50% overlap with nperseg == nfft: the half-block kernel (each half-block loaded once, window
+  // fused into the first butterfly stage) for no / constant detrend
+  const bool half = kind != kFrameCross && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
+  if (half) {
+    const int hdet = spectral ? 2 : detrend;
+    const FrameInfo fh = kind == kFrameStft ? frame_half_lookup_stft(log_l, hdet)
+                                            : frame_half_lookup_power(log_l, hdet);
+    if (fh.fn != nullptr) f = fh;
+  }
   const int nseg = int((n_total - nperseg) / hop + 1);
   const int64_t total = rows * nseg;
   if (total == 0) return SP_OK;

@@ -63,6 +63,9 @@ FrameInfo frame_lookup_power(int log_l, int det);
 FrameInfo frame_lookup_stft_spectral(int log_l);   // constant detrend, spectral correction
 FrameInfo frame_lookup_power_spectral(int log_l);
 FrameInfo frame_lookup_cross(int log_l, int det);
+// hop == nperseg/2 == nfft/2, nfft >= 64 (empty info below); det 0/1/2(spectral)
+FrameInfo frame_half_lookup_stft(int log_l, int det);
+FrameInfo frame_half_lookup_power(int log_l, int det);
 
 // Fold-expression lookup over LOG_L = 0..kMaxLogL and detrend 0..2 of an info factory.
 template <class INFO, template <int, int> class F, int... LS>

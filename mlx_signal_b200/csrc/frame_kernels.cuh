@@ -183,4 +183,195 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Per-frame spectra for hop == nperseg/2 == nfft/2 (stft's and the bench spectrogram's case).
+// The structure of welch_half_range (mean_kernels.cuh): a frame pair (s, s+1) spans half-blocks
+// A | B | C of the extended signal, each half-block is loaded once (C is carried into the next
+// pair as its A) and the window multiply is fused into the first radix-2 stage. Differences:
+// half-blocks that touch the boundary extension or the zero padding are read through
+// ext_sample (virtual extension), and every pair ends in the per-frame untangle and store of
+// k_frames instead of a power accumulation. DET: kDetrendNone, kDetrendConstant (time domain,
+// from the half-block sums) or kDetrendConstantSpectral (low-bin correction after the FFT).
+// ------------------------------------------------------------------------------------------
+template <class PL, int KIND, int DET, bool WT>
+__device__ __forceinline__ void frames_half_range(const HalfCtx<PL>& c, const FrameParams& pr,
+                                                  int64_t r, int s0, int s1) {
+  constexpr int L = PL::L, E = PL::E, P = PL::P, H = L / 2, EH = E / 2;
+  constexpr int R0 = PL::radix(0), B0 = E / R0;
+  const int t = c.t;
+  const float* __restrict__ xr = pr.x + r * pr.ld_x;
+  const float inv_n = 1.0f / float(L);
+  const bool onesided = pr.nbins != L || L == 1;
+  float A[EH], B[EH], C[EH];
+  bool carry = false;
+  float sum_c = 0.f;
+  // half-block j of the extended signal: samples j*H + n, n in [0, H)
+  auto load_block = [&](float (&dst)[EH], int64_t j) {
+    const int64_t p0 = j * H - pr.ext;  // index of the block start in the original row
+    if (p0 >= 0 && p0 + H <= pr.n) {
+      static_for<0, EH>([&](auto gc) {
+        constexpr int gi = decltype(gc)::value;
+        dst[gi] = __ldg(xr + p0 + slot_elem<PL, 2 * gi>(t));
+      });
+    } else {
+      static_for<0, EH>([&](auto gc) {
+        constexpr int gi = decltype(gc)::value;
+        dst[gi] = ext_sample(xr, pr.n, pr.ext, pr.ext_mode, j * H + slot_elem<PL, 2 * gi>(t));
+      });
+    }
+  };
+  auto step = [&](int s, auto two_c) {
+    const bool TWO = bool(two_c);
+    {  // warm L2 with the next pair's two new half-blocks when they lie inside the row
+      const int64_t lo = int64_t(s + 3) * H - pr.ext, hi = lo + 2 * H;
+      if (s + 3 < s1 && lo >= 0 && hi <= pr.n) {
+        for (int o = t * 32; o < 2 * H; o += P * 32)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(xr + lo + o));
+      }
+    }
+    if (!carry) load_block(A, s);
+    load_block(B, s + 1);
+    if (TWO) {
+      load_block(C, s + 2);
+    } else {
+#pragma unroll
+      for (int i = 0; i < EH; ++i) C[i] = 0.f;
+    }
+    float ma = 0.f, mb = 0.f;
+    if constexpr (DET == kDetrendConstant || DET == kDetrendConstantSpectral) {
+      float sa = sum_c;
+      if (!carry) {
+        float sums[1] = {tree_sum<EH>([&](auto gc) { return A[decltype(gc)::value]; })};
+        team_sum<P, 1>(sums, c.scratch, c.mask);
+        sa = sums[0];
+      }
+      float sums[2] = {tree_sum<EH>([&](auto gc) { return B[decltype(gc)::value]; }),
+                       TWO ? tree_sum<EH>([&](auto gc) { return C[decltype(gc)::value]; })
+                           : 0.f};
+      team_sum<P, 2>(sums, c.scratch, c.mask);
+      ma = (sa + sums[0]) * inv_n;
+      mb = TWO ? (sums[0] + sums[1]) * inv_n : 0.f;
+      sum_c = sums[1];
+    }
+    float2 v[E];
+    auto fuse = [&](auto gc, float wl, float wh) {
+      constexpr int gi = decltype(gc)::value;
+      float2 zl = make_float2(A[gi], TWO ? B[gi] : 0.f);
+      float2 zh = make_float2(B[gi], C[gi]);
+      if constexpr (DET == kDetrendConstant) {
+        zl = make_float2(zl.x - ma, TWO ? zl.y - mb : 0.f);
+        zh = make_float2(zh.x - ma, TWO ? zh.y - mb : 0.f);
+      }
+      const float2 a = make_float2(zl.x * wl, zl.y * wl);
+      v[2 * gi] = make_float2(fmaf(zh.x, wh, a.x), fmaf(zh.y, wh, a.y));
+      v[2 * gi + 1] = make_float2(fmaf(-zh.x, wh, a.x), fmaf(-zh.y, wh, a.y));
+    };
+    if constexpr (WT) {
+      static_for<0, EH / 2>([&](auto pc) {
+        constexpr int gp = decltype(pc)::value;
+        const float4 w4 = c.wt[gp];
+        fuse(std::integral_constant<int, 2 * gp>{}, w4.x, w4.y);
+        fuse(std::integral_constant<int, 2 * gp + 1>{}, w4.z, w4.w);
+      });
+    } else {
+      static_for<0, EH>([&](auto gc) {
+        constexpr int gi = decltype(gc)::value;
+        const int n = slot_elem<PL, 2 * gi>(t);
+        fuse(gc, c.win[n], c.win[n + H]);
+      });
+    }
+    static_for<0, B0>([&](auto bc) {
+      constexpr int b = decltype(bc)::value;
+      dft_dit<R0, b * R0, 2>(v);
+    });
+    team_passes<PL>(v, c.buf, c.tw, t, c.mask);
+    if constexpr (DET == kDetrendConstantSpectral) {
+      const float2 m = make_float2(ma, mb);
+      v[0] = csub(v[0], cmul(m, c.wlo[t]));
+      v[E - 1] = csub(v[E - 1], cmul(m, c.whi[t]));
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
+    team_sync<P>(c.mask);
+    const int64_t fa = r * pr.nseg + s;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = t + e * P;
+      if (k < pr.nbins) {
+        const float2 z = v[e];
+        const float2 m = c.buf[PL::pad((L - k) & (L - 1))];
+        const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
+        const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+        if constexpr (KIND == kFrameStft) {
+          float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
+          oa[k] = xa;
+          if (TWO) oa[pr.nbins + k] = xb;
+        } else {
+          const float f = (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f;
+          float* oa = pr.out + fa * pr.nbins;
+          oa[k] = f * fmaf(xa.x, xa.x, xa.y * xa.y);
+          if (TWO) oa[pr.nbins + k] = f * fmaf(xb.x, xb.x, xb.y * xb.y);
+        }
+      }
+    }
+    team_sync<P>(c.mask);
+#pragma unroll
+    for (int i = 0; i < EH; ++i) A[i] = C[i];
+    carry = true;
+  };
+  int s = s0;
+  for (; s + 1 < s1; s += 2) step(s, std::true_type{});
+  if (s < s1) step(s, std::false_type{});
+}
+
+template <int LOG_L, int LOG_E, int KIND, int DET>
+__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L, LOG_E>::MIN_CTAS)
+    k_frames_half(FrameParams pr) {
+  using CFG = MeanCfg<LOG_L, LOG_E>;
+  using PL = typename CFG::PL;
+  constexpr int L = PL::L, P = PL::P;
+  constexpr bool WT = HalfWinT<PL>::USE;
+  extern __shared__ float4 smem[];
+  float* win1 = reinterpret_cast<float*>(smem + CFG::TEAMS * CFG::SCRATCH);
+  float2* wlo = reinterpret_cast<float2*>(win1 + HalfSmem<CFG>::WINF);
+  float2* whi = wlo + P;
+  float2* tw = whi + P;
+  float2* sbuf = tw + PL::TW;
+  if constexpr (WT) {
+    build_half_wint<PL>(win1, pr.win, threadIdx.x);
+  } else {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) win1[i] = pr.win[i];
+  }
+  if constexpr (DET == kDetrendConstantSpectral)
+    load_window_lowbins<P>(wlo, whi, pr.wdft, pr.n_low, threadIdx.x, blockDim.x);
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / P;
+  HalfCtx<PL> c;
+  c.win = win1;
+  c.wt = reinterpret_cast<const float4*>(win1) +
+         (threadIdx.x - team * P) * (HalfWinT<PL>::WS / 4);
+  c.wlo = wlo;
+  c.whi = whi;
+  c.tw = tw;
+  c.buf = sbuf + team * PL::BUF;
+  c.scratch = smem + team * CFG::SCRATCH;
+  c.t = threadIdx.x - team * P;
+  c.mask = team_mask<P>();
+  const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
+  const int64_t nt = int64_t(gridDim.x) * CFG::TEAMS;
+  const int64_t G = (pr.total + nt - 1) / nt;
+  const int64_t Ge = G + (G & 1);
+  int64_t g = tau * Ge;
+  const int64_t gend = min(g + Ge, pr.total);
+  while (g < gend) {
+    const int64_t r = g / pr.nseg;
+    const int s0 = int(g - r * pr.nseg);
+    const int64_t lim = int64_t(s0) + (gend - g);
+    const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
+    frames_half_range<PL, KIND, DET, WT>(c, pr, r, s0, s1);
+    g += s1 - s0;
+  }
+}
+
 }  // namespace b2s

@@ -328,3 +328,48 @@ def test_istft_plan_repeats_and_warns(rng):
     for _ in range(2):
         with pytest.warns(UserWarning, match="NOLA"):
             msig.istft(z, window=("tukey", 0.9), nperseg=256, noverlap=0)
+
+
+# 50%-overlap per-frame kernel (k_frames_half): boundary extension, padding, detrend variants
+@pytest.mark.parametrize("nperseg", [64, 256, 1024, 2048, 4096])
+@pytest.mark.parametrize("boundary,padded", [("zeros", True), ("even", True), ("odd", False),
+                                             ("constant", True), (None, False), (None, True)])
+def test_half_overlap_stft_matches_scipy(rng, nperseg, boundary, padded):
+    n = 3 * nperseg + 37
+    x = make_sig(rng, (3, n))
+    x[1] += 3.0  # a DC offset exercises the detrend variants
+    for detrend in (False, "constant"):
+        kw = dict(nperseg=nperseg, boundary=boundary, padded=padded, detrend=detrend)
+        f_ref, t_ref, z_ref = sps.stft(x.astype(np.float64), **kw)
+        f, t, z = msig.stft(x, **kw)
+        assert tuple(z.shape) == z_ref.shape
+        assert_close(t, t_ref)
+        assert_close(z, z_ref)
+
+
+@pytest.mark.parametrize("nperseg", [64, 512, 1024, 4096])
+@pytest.mark.parametrize("detrend", [False, "constant"])
+@pytest.mark.parametrize("mode", ["psd", "complex", "magnitude"])
+def test_half_overlap_spectrogram_matches_scipy(rng, nperseg, detrend, mode):
+    x = make_sig(rng, (2, 5 * nperseg + 11))
+    x[0] += 2.0
+    kw = dict(nperseg=nperseg, noverlap=nperseg // 2, window="hann", detrend=detrend, mode=mode)
+    f_ref, t_ref, s_ref = sps.spectrogram(x.astype(np.float64), **kw)
+    f, t, s = msig.spectrogram(x, **kw)
+    assert tuple(s.shape) == s_ref.shape
+    assert_close(s, s_ref)
+    # tukey window: its spectrum is not confined to low bins -> time-domain constant detrend
+    kw["window"] = ("tukey", 0.25)
+    f_ref, t_ref, s_ref = sps.spectrogram(x.astype(np.float64), **kw)
+    assert_close(msig.spectrogram(x, **kw)[2], s_ref)
+
+
+def test_half_overlap_single_and_odd_frame_counts(rng):
+    for n, nperseg in [(1024, 1024), (1536, 1024), (2048, 1024), (64, 64), (97, 64)]:
+        x = make_sig(rng, (2, n))
+        for padded in (False, True):
+            _, _, z_ref = sps.stft(x.astype(np.float64), nperseg=nperseg, boundary=None,
+                                   padded=padded)
+            _, _, z = msig.stft(x, nperseg=nperseg, boundary=None, padded=padded)
+            assert tuple(z.shape) == z_ref.shape
+            assert_close(z, z_ref)
