@@ -479,11 +479,55 @@ def secondary(x, steps, warmup, dist, clocks):
 
         cpu_reference.close_pool()
     del y, z, xr
+    out["general_shapes"] = general_shapes(x, dist, clocks, peak)
     out["batched_512_uneven"] = batched_uneven(dist, clocks, peak)
     out["rfft_1x2p23"] = large_rfft(dist, clocks, peak)
     out["fft_consumers"] = fft_consumers(dist, clocks, peak)
     out["reference_published_rows"] = published_rows(dist, clocks)
     return out
+
+
+def general_shapes(x, dist, clocks, peak):
+    """welch and stft on the 64 x 2^20 input with a non-power-of-two nperseg (1000): fused
+    Bluestein kernels; the composed path (strided frames + cuFFT) timed beside them, and the
+    accuracy against float64 scipy on two channels."""
+    import torch
+    import scipy.signal as sps
+
+    import mlx_signal_b200 as msig
+    from mlx_signal_b200 import _kernels
+
+    res = {}
+    nps = 1000
+    nseg = (NSAMP - nps) // (nps // 2) + 1
+    b = C * NSAMP * 4 + C * (nps // 2 + 1) * 4
+    ms = timed(lambda: msig.welch(x, fs=FS, nperseg=nps), 10, 3, dist, clocks)
+    # the same call on the composed path (what non-power-of-two shapes cost without the kernels)
+    win = torch.from_numpy(sps.get_window("hann", nps).astype(np.float32)).to(x.device)
+
+    def composed():
+        fr = x.unfold(-1, nps, nps // 2)
+        fr = (fr - fr.mean(dim=-1, keepdim=True)) * win
+        return torch.fft.rfft(fr, dim=-1).abs().square().mean(dim=-2)
+
+    ms_c = timed(composed, 5, 2, dist, clocks)
+    res["welch_64x2p20_n1000"] = {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
+                                  "composed_cufft_ms": ms_c,
+                                  "kernel": "k_blue_welch<11> (M = 2048 chirp-z)"}
+    x16 = x[:16]
+    nf = (NSAMP + nps - nps) // (nps // 2) + 1
+    bs = 16 * NSAMP * 4 + 16 * nf * (nps // 2 + 1) * 8
+    ms = timed(lambda: msig.stft(x16, fs=FS, nperseg=nps), 10, 3, dist, clocks)
+    res["stft_16x2p20_n1000"] = {"ms": ms, "GB/s": bs / ms / 1e6, "frac_hbm": bs / ms / 1e6 / peak}
+    if dist is None:
+        xs = x[:2].cpu().numpy().astype(np.float64)
+        _, p_ref = sps.welch(xs, fs=FS, nperseg=nps)
+        _, p = msig.welch(x[:2], fs=FS, nperseg=nps)
+        p = p.cpu().numpy()
+        m = p_ref > 1e-6 * p_ref.max(axis=-1, keepdims=True)
+        res["welch_64x2p20_n1000"]["max_rel_err"] = float(np.max(np.abs(p - p_ref)[m] / p_ref[m]))
+    _ = nseg, _kernels
+    return res
 
 
 #: the reference's published device times for this path (Apple M4 Max, MLX 0.32.2, float32;

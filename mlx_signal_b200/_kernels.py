@@ -28,6 +28,15 @@ def fused_mean_ok(nfft: int) -> bool:
     return is_pow2(nfft) and nfft <= MAX_FUSED_NFFT
 
 
+#: longest non-power-of-two nfft the Bluestein kernels take (welch, stft, spectrogram)
+MAX_BLUE_NFFT = 2048
+
+
+def blue_ok(nfft: int) -> bool:
+    """A non-power-of-two nfft the Bluestein (chirp-z) kernels compute fused."""
+    return not is_pow2(nfft) and 3 <= nfft <= MAX_BLUE_NFFT
+
+
 def _rows(x: torch.Tensor) -> tuple[torch.Tensor, int]:
     """2-D float32 CUDA view with unit inner stride; returns (tensor, row stride)."""
     assert x.dim() == 2 and x.is_cuda and x.dtype == torch.float32

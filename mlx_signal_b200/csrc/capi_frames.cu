@@ -35,18 +35,30 @@ int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n
     return SP_ERR_ARG;
   }
   const int log_l = ilog2_exact(nfft);
-  if (log_l < 0 || log_l > kMaxLogL) {
-    set_error("nfft=%d: fused kernels need a power of two <= %d", nfft, 1 << kMaxLogL);
+  // stft / spectrogram with a non-power-of-two nfft: the Bluestein frame kernels
+  const bool blue = log_l < 0 && kind != kFrameCross && nfft >= 3 && nfft <= kBlueMaxN;
+  if (!blue && (log_l < 0 || log_l > kMaxLogL)) {
+    set_error("nfft=%d: fused kernels need a power of two <= %d (stft/spectrogram: or any "
+              "nfft <= %d)", nfft, 1 << kMaxLogL, kBlueMaxN);
     return SP_ERR_UNSUPPORTED;
   }
   // the spectral correction applies to the constant detrend when the window's spectrum is
   // confined to bins a team thread holds in its first and last register
-  const bool spectral = kind != kFrameCross && detrend == kDetrendConstant && wdft != nullptr &&
-                        n_low >= 1 && n_low <= ((1 << log_l) >> team_log_e_rt(log_l));
-  FrameInfo f = lookup(kind, log_l, detrend, spectral);
+  const bool spectral = !blue && kind != kFrameCross && detrend == kDetrendConstant &&
+                        wdft != nullptr && n_low >= 1 &&
+                        n_low <= ((1 << log_l) >> team_log_e_rt(log_l));
+  FrameInfo f;
+  if (blue) {
+    const int lm = blue_log_m(nfft);
+    f = kind == kFrameStft ? blue_lookup_frames_stft(lm, detrend)
+                           : blue_lookup_frames_power(lm, detrend);
+  } else {
+    f = lookup(kind, log_l, detrend, spectral);
+  }
   // 50% overlap with nperseg == nfft: the half-block kernel (each half-block loaded once, window
   // fused into the first butterfly stage) for no / constant detrend
-  const bool half = kind != kFrameCross && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
+  const bool half = !blue && kind != kFrameCross && nperseg == nfft && 2 * hop == nperseg &&
+                    detrend <= 1;
   if (half) {
     const int hdet = spectral ? 2 : detrend;
     const FrameInfo fh = kind == kFrameStft ? frame_half_lookup_stft(log_l, hdet)
@@ -89,6 +101,7 @@ int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n
   p.out3 = nullptr;
   p.wdft = spectral ? reinterpret_cast<const float2*>(wdft) : nullptr;
   p.n_low = spectral ? n_low : 0;
+  p.nfft = nfft;
   f.launch(dim3(unsigned(blocks)), f.threads, f.smem, static_cast<cudaStream_t>(stream), p);
   B2S_CHECK_CUDA(cudaGetLastError(), "frame kernel launch");
   return SP_OK;

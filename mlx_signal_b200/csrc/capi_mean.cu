@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p)
   const int k = int(blockIdx.x - r * chunks) * 32 + lane;
   const bool live = k < p.nout;
   const int L = p.L;
-  const int kk = (L - k) & (L - 1);
+  const int kk = k == 0 ? 0 : L - k;  // mirror bin of the L-periodic spectrum (any L)
   const int kc = k <= kk ? k : kk;
   const int64_t t0 = first_team(r, p.nseg, p.G);
   int64_t t1 = last_team(r, p.nseg, p.G);
@@ -121,15 +121,21 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
               (long long)rows, (long long)n, nperseg, nfft, hop);
     return SP_ERR_ARG;
   }
-  const int log_l = ilog2_exact(nfft);
-  if (log_l < 0 || log_l > kMaxLog) {
-    set_error("nfft=%d: fused kernels need a power of two <= %d", nfft, 1 << kMaxLog);
+  int log_l = ilog2_exact(nfft);
+  // welch with a non-power-of-two nfft: the Bluestein kernel on a power-of-two transform
+  const bool blue = log_l < 0 && !cross && nfft >= 3 && nfft <= kBlueMaxN;
+  if (!blue && (log_l < 0 || log_l > kMaxLog)) {
+    set_error("nfft=%d: fused kernels need a power of two <= %d (welch: or any nfft <= %d)",
+              nfft, 1 << kMaxLog, kBlueMaxN);
     return SP_ERR_UNSUPPORTED;
   }
-  const bool half = log_l >= 1 && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
+  if (blue) log_l = blue_log_m(nfft);
+  const bool half = !blue && log_l >= 1 && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
   const int hdet = (spectral && detrend == 1) ? 2 : detrend;  // lookup index: 2 = spectral
   MeanInfo canon;
-  if (cross && half) {
+  if (blue) {
+    pl->k = canon = blue_lookup_welch(log_l, detrend);
+  } else if (cross && half) {
     pl->k = mean_lookup_cross_half(log_l, hdet, mode == 1);
     canon = mean_lookup_cross_half(log_l, detrend, false);
   } else if (cross) {
@@ -162,8 +168,7 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   int64_t cm = cdiv(pl->nseg, pl->G) + 1;
   if (cm > pl->nteams) cm = pl->nteams;
   pl->cmax = int(cm);
-  const int64_t L = int64_t(1) << log_l;
-  pl->slot_floats = cross ? cross_slot_floats(int(L)) : welch_slot_floats(int(L));
+  pl->slot_floats = cross ? cross_slot_floats(nfft) : welch_slot_floats(nfft);
   pl->ws_bytes = rows * pl->cmax * pl->slot_floats * int64_t(sizeof(float));
   return SP_OK;
 }
@@ -207,6 +212,7 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   // the spectral tables are read only by the 50%-overlap kernels' spectral variants
   p.wdft = spectral ? reinterpret_cast<const float2*>(wdft) : nullptr;
   p.n_low = spectral ? n_low : 0;
+  p.nfft = nfft;
   pl.k.launch(dim3(unsigned(pl.blocks)), pl.k.threads, pl.k.smem, s, p);
   B2S_CHECK_CUDA(cudaGetLastError(), "spectral-mean kernel launch");
   ReduceParams rp;

@@ -6,6 +6,7 @@
 
 #include <utility>
 
+#include "blue_kernels.cuh"
 #include "frame_kernels.cuh"
 #include "istft_kernels.cuh"
 #include "mean_kernels.cuh"
@@ -63,6 +64,17 @@ FrameInfo frame_lookup_power(int log_l, int det);
 FrameInfo frame_lookup_stft_spectral(int log_l);   // constant detrend, spectral correction
 FrameInfo frame_lookup_power_spectral(int log_l);
 FrameInfo frame_lookup_cross(int log_l, int det);
+// Bluestein kernels for a non-power-of-two nfft in [3, kBlueMaxN]: transform length
+// M = 2^log_m >= 2 nfft - 1 (log_m in [4, 12]); det 0 none, 1 constant, 2 linear.
+constexpr int kBlueMaxN = 2048;
+inline int blue_log_m(int nfft) {
+  int lm = 4;
+  while ((1 << lm) < 2 * nfft - 1) ++lm;
+  return lm;
+}
+MeanInfo blue_lookup_welch(int log_m, int det);
+FrameInfo blue_lookup_frames_stft(int log_m, int det);
+FrameInfo blue_lookup_frames_power(int log_m, int det);
 // hop == nperseg/2 == nfft/2, nfft >= 64 (empty info below); det 0/1/2(spectral)
 FrameInfo frame_half_lookup_stft(int log_l, int det);
 FrameInfo frame_half_lookup_power(int log_l, int det);

@@ -22,6 +22,7 @@ struct MeanParams {
   float* partial;      // workspace: [rows][cmax][slot_floats]
   const float2* wdft;  // DFT_L(win)[0..n_low) for the spectral detrend correction, else nullptr
   int n_low;           // bins of the window spectrum that are non-zero: |k| < n_low (mod L)
+  int nfft;            // DFT length (the Bluestein kernels' N; equals L for the others)
 };
 
 // Per-frame kernels (stft / spectrogram / per-frame cross spectra).
@@ -46,6 +47,7 @@ struct FrameParams {
   float* out3;         // third output (per-frame pxy), else nullptr
   const float2* wdft;  // DFT_nfft(win)[0..n_low) for the spectral constant detrend, else nullptr
   int n_low;
+  int nfft;            // DFT length (the Bluestein kernels' N; equals L for the others)
 };
 
 }  // namespace b2s

@@ -8,8 +8,9 @@ complex64). Computation is float32/complex64.
 Routing (the reference's `_stft_metal.eligible` rule, spectral.py:319-347, widened): real
 float32 input with a power-of-two nfft <= 4096 and detrend in {False, 'constant', 'linear'}
 runs the fused CUDA kernels (segment gather + detrend + window + FFT + |X|^2 or X conj(Y) +
-segment mean in one sweep). Other shapes (non-power-of-two nfft, complex input, median
-averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
+segment mean in one sweep); welch, stft and spectrogram with any other nfft <= 2048 run fused
+Bluestein (chirp-z) kernels. Other shapes (larger non-power-of-two nfft, non-power-of-two csd /
+coherence of two signals, complex input, median averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
 counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing runs on the CPU.
 """
 
@@ -273,8 +274,8 @@ def _setup_same(key, x, fs, window, nperseg, noverlap, nfft, detrend, return_one
     s = _setup(x, x, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
                axis, mode, boundary, padded, True)
     requested = 256 if nperseg is None else int(nperseg)
-    if (key is not None and s.empty is None and s.fused and isinstance(window, str | tuple)
-            and requested <= s.n_orig):
+    if (key is not None and s.empty is None and (s.fused or s.blue)
+            and isinstance(window, str | tuple) and requested <= s.n_orig):
         _remember_setup(key, s)
     return s
 
@@ -360,6 +361,8 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
     s.win = device_vector((win_np * np.sqrt(scale)).astype(np.float32))
     s.freqs = _freqs(nfft, fs, onesided)
     s.fused = (not x_complex) and (not y_complex) and _kernels.fused_mean_ok(nfft)
+    # non-power-of-two nfft: Bluestein kernels for welch / stft / spectrogram (same-input kinds)
+    s.blue = (not x_complex) and (not y_complex) and _kernels.blue_ok(nfft)
     return s
 
 
@@ -506,7 +509,7 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     outer = tuple(X.shape[:-1]) if same else s.outershape
     n = X.shape[-1]
     nseg = (n - s.nperseg) // s.nstep + 1
-    if s.fused and average == "mean":
+    if average == "mean" and (s.fused or (same and s.blue)):
         rows = int(np.prod(outer)) if outer else 1
         if same:
             res = _kernels.welch_mean(X.reshape(rows, n), s.win, s.nperseg, s.nfft, s.nstep,
@@ -650,7 +653,7 @@ def coherence(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=Non
 def _frames_result(s, mode: str) -> torch.Tensor:
     """Per-frame spectra (..., nseg, nfreq): complex (stft) or power (psd)."""
     X = s.X
-    if s.fused:
+    if s.fused or s.blue:
         outer = tuple(X.shape[:-1])
         rows = int(np.prod(outer)) if outer else 1
         n = X.shape[-1]
@@ -689,7 +692,7 @@ def spectrogram(x, fs=1.0, window=("tukey", 0.25), nperseg=None, noverlap=None, 
             noverlap = nperseg // 8
         s = _setup(X, X, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, scaling,
                    axis, helper_mode, None, False, True)
-        if (key is not None and s.empty is None and s.fused
+        if (key is not None and s.empty is None and (s.fused or s.blue)
                 and (256 if req is None else int(req)) <= s.n_orig):
             _remember_setup(key, s)
     if s.empty is not None:

@@ -373,3 +373,30 @@ def test_half_overlap_single_and_odd_frame_counts(rng):
             _, _, z = msig.stft(x, nperseg=nperseg, boundary=None, padded=padded)
             assert tuple(z.shape) == z_ref.shape
             assert_close(z, z_ref)
+
+
+# non-power-of-two nfft: fused Bluestein frame kernels
+@pytest.mark.parametrize("kw", [{"nperseg": 1000}, {"nperseg": 300, "noverlap": 123},
+                                {"nperseg": 77, "nfft": 81, "boundary": "even"},
+                                {"nperseg": 500, "detrend": "constant", "boundary": None,
+                                 "padded": False},
+                                {"nperseg": 1500, "detrend": "linear", "boundary": "odd"},
+                                {"nperseg": 6, "return_onesided": False}])
+def test_bluestein_stft_matches_scipy(rng, kw):
+    x = make_sig(rng, (2, 7001))
+    x[1] += 2.0
+    f_ref, t_ref, z_ref = sps.stft(x.astype(np.float64), **kw)
+    f, t, z = msig.stft(x, **kw)
+    assert tuple(z.shape) == z_ref.shape
+    assert_close(f, f_ref)
+    assert_close(z, z_ref)
+
+
+@pytest.mark.parametrize("mode", ["psd", "complex", "magnitude", "phase"])
+def test_bluestein_spectrogram_matches_scipy(rng, mode):
+    x = make_sig(rng, (3, 9000))
+    kw = dict(nperseg=441, noverlap=220, mode=mode, fs=44100.0)
+    f_ref, t_ref, s_ref = sps.spectrogram(x.astype(np.float64), **kw)
+    f, t, s = msig.spectrogram(x, **kw)
+    assert tuple(s.shape) == s_ref.shape
+    assert_close(s, s_ref, rtol=1e-3 if mode == "phase" else 1e-4)

@@ -318,3 +318,29 @@ def test_welch_plan_cache_keeps_warnings_and_errors(rng):
     msig.welch(xt, detrend=False, nperseg=128)
     with pytest.raises(ValueError):
         msig.welch(xt, detrend=0, nperseg=128)
+
+
+# non-power-of-two nfft: fused Bluestein (chirp-z) kernels
+@pytest.mark.parametrize("kw", [{"nperseg": 1000}, {"nperseg": 768, "noverlap": 100},
+                                {"nperseg": 100, "nfft": 150}, {"nperseg": 3},
+                                {"nperseg": 2047, "detrend": "linear"},
+                                {"nperseg": 999, "detrend": False, "scaling": "spectrum"},
+                                {"nperseg": 300, "return_onesided": False},
+                                {"nperseg": 129, "window": ("tukey", 0.3), "fs": 44.1}])
+def test_bluestein_welch_matches_scipy(rng, kw):
+    x = make_sig(rng, (3, 20000))
+    x[0] += 1.5
+    f_ref, p_ref = sps.welch(x.astype(np.float64), **kw)
+    f, p = msig.welch(x, **kw)
+    assert tuple(p.shape) == p_ref.shape
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+    assert rel_err_bins(p, p_ref) <= 1e-5
+
+
+def test_bluestein_welch_north_star_shape(rng):
+    """64 x 2^18 channels, nperseg 1000: the 1e-5 bar on bins above 1e-6 of the peak."""
+    x = make_sig(rng, (64, 1 << 18))
+    f_ref, p_ref = sps.welch(x.astype(np.float64), fs=48000, nperseg=1000)
+    f, p = msig.welch(torch.from_numpy(x).cuda(), fs=48000, nperseg=1000)
+    assert rel_err_bins(p, p_ref) <= 1e-5
