@@ -114,3 +114,10 @@ def test_conv_ols_block_choice_and_argument_errors():
     assert lib.sp_conv_ols_f32(dummy, 1, 4000, 4000, dummy, 2050, 0, 10, dummy, 10, None) == \
         _lib.SP_ERR_UNSUPPORTED
     assert lib.sp_conv_ols_f32(dummy, 0, 100, 100, dummy, 10, 0, 109, dummy, 109, None) == _lib.SP_OK
+
+
+def test_profiling_workloads_listed():
+    from mlx_signal_b200 import workloads
+
+    assert workloads.main(["--list"]) == 0
+    assert {"welch_64x2p20_n1024", "conv_8x2p22_t1025", "rfft_2p23"} <= set(workloads.WORKLOADS)
