@@ -52,8 +52,8 @@ SP_API int sp_version(void);
 SP_API const char* sp_last_error(void);
 
 /*
- * Workspace bytes for sp_welch_f32 (kind 0) or sp_csd_c64 / sp_coherence_f32 (kind 1) on the
- * current device. Negative return = error status.
+ * Workspace bytes for sp_welch_f32 (kind 0), sp_csd_c64 / sp_coherence_f32 (kind 1) or
+ * sp_welch_c64 (kind 3) on the current device. Negative return = error status.
  * Replaces the implicit group-partial buffers of _stft_metal.rfft_power_mean
  * (_stft_metal.py:530-557) and _pair_sum_launch (_stft_metal.py:703-736).
  */
@@ -63,13 +63,26 @@ SP_API int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int npe
 /*
  * Welch PSD: out[r][k] = (onesided ? f_k : 1) / nseg * sum_s |FFT_nfft(win * detrend(x_rs))_k|^2
  * for k < (onesided ? nfft/2+1 : nfft), segments x_rs = x[r, s*hop : s*hop+nperseg].
- * nfft must be a power of two in [1, 4096] with nperseg <= nfft; win holds nperseg values.
+ * nfft: a power of two in [1, 4096], or any other value in [3, 2048] (chirp-z kernels), with
+ * nperseg <= nfft; win holds nperseg values.
  * Replaces _stft_metal.rfft_power_mean (_stft_metal.py:530-557) together with the deferred
- * one-sided factor of spectral.csd (spectral.py:468-488).
+ * one-sided factor of spectral.csd (spectral.py:468-488); for a non-power-of-two nfft the composed
+ * frames + mx.fft.rfft path of spectral._fft_frames (spectral.py:127-147).
  */
 SP_API int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
                  int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
                  void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Welch PSD of complex rows (x interleaved complex64, ld in complex elements), two-sided:
+ * out[r][k] = 1/nseg * sum_s |FFT_nfft(win * detrend(x_rs))_k|^2, k < nfft; the detrend acts on
+ * the real and imaginary parts separately. nfft a power of two in [1, 4096]. Workspace:
+ * sp_mean_workspace_size(3, ...). Replaces the composed complex path of spectral.csd
+ * (spectral.py:290-298 two-sided switch, :127-147 frames + mx.fft.fft).
+ */
+SP_API int sp_welch_c64(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
+                        int nperseg, int nfft, int hop, int detrend, float* out, void* workspace,
+                        size_t workspace_bytes, void* stream);
 
 /*
  * sp_welch_f32 with the constant detrend applied in the frequency domain. `win_dft_low` is a
@@ -141,6 +154,17 @@ SP_API int sp_coherence_f32_ex(const float* x, const float* y, int64_t rows, int
                                int hop, int detrend, float* out, void* workspace,
                                size_t workspace_bytes, void* stream);
 
+
+/*
+ * Per-frame spectra of complex rows (x interleaved complex64, ld in complex elements), two-sided:
+ * out (rows, nseg, nfft) complex64 X_s (power = 0) or float32 |X_s|^2 (power = 1), with the same
+ * boundary extension / padding arguments as sp_stft_c64; nfft a power of two in [1, 4096].
+ * Replaces the composed complex path of spectral._fft_frames (spectral.py:127-147) used by
+ * stft / spectrogram on complex input.
+ */
+SP_API int sp_frames_cplx(const float* x, int64_t rows, int64_t n, int64_t ld, int ext,
+                          int ext_mode, int64_t n_total, const float* win, int nperseg, int nfft,
+                          int hop, int detrend, int power, float* out, void* stream);
 
 /* Boundary extension modes of the per-frame entry points (scipy stft `boundary`). */
 enum { SP_EXT_NONE = 0, SP_EXT_ZEROS = 1, SP_EXT_EVEN = 2, SP_EXT_ODD = 3, SP_EXT_CONSTANT = 4 };

@@ -259,3 +259,50 @@ def conv_ols(x: torch.Tensor, h: torch.Tensor, j0: int, nout: int) -> torch.Tens
         "sp_conv_ols_f32",
     )
     return out
+
+
+def _rows_c(x: torch.Tensor) -> tuple[torch.Tensor, int]:
+    """2-D complex64 CUDA view with unit inner stride; returns (tensor, row stride in complex
+    elements)."""
+    assert x.dim() == 2 and x.is_cuda and x.dtype == torch.complex64
+    if x.stride(1) != 1 or (x.shape[0] > 1 and x.stride(0) < x.shape[1]):
+        x = x.contiguous()
+    ld = x.stride(0) if x.shape[0] > 1 else x.shape[1]
+    return x, max(int(ld), x.shape[1])
+
+
+def welch_mean_complex(x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop: int,
+                       detrend: int) -> torch.Tensor:
+    """Two-sided mean |FFT(win * detrend(segment))|^2 over the segments of each complex row of x
+    -> (rows, nfft) float32 (power-of-two nfft)."""
+    x, ld = _rows_c(x)
+    rows, n = x.shape
+    lib = _lib.load()
+    ws_bytes = lib.sp_mean_workspace_size(3, rows, n, nperseg, nfft, hop, detrend)
+    if ws_bytes < 0:
+        _lib.check(int(ws_bytes), "sp_mean_workspace_size")
+    out = torch.empty((rows, nfft), dtype=torch.float32, device=x.device)
+    ws = _workspace(ws_bytes, x.device)
+    _lib.check(lib.sp_welch_c64(x.data_ptr(), rows, n, ld, win.data_ptr(), nperseg, nfft, hop,
+                                detrend, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                stream_handle()), "sp_welch_c64")
+    return out
+
+
+def frames_complex(kind: str, x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int,
+                   hop: int, detrend: int, ext: int = 0, ext_mode=None,
+                   n_total: int | None = None) -> torch.Tensor:
+    """Per-frame two-sided spectra of complex rows: (rows, nseg, nfft) complex64 ('stft') or
+    float32 |X|^2 ('power'); boundary extension and padding virtual, as in `frames`."""
+    x, ld = _rows_c(x)
+    rows, n = x.shape
+    n_total = n + 2 * ext if n_total is None else int(n_total)
+    nseg = (n_total - nperseg) // hop + 1
+    power = kind == "power"
+    out = torch.empty((rows, nseg, nfft), dtype=torch.float32 if power else torch.complex64,
+                      device=x.device)
+    _lib.check(_lib.load().sp_frames_cplx(x.data_ptr(), rows, n, ld, ext, EXT_CODES[ext_mode],
+                                          n_total, win.data_ptr(), nperseg, nfft, hop, detrend,
+                                          int(power), out.data_ptr(), stream_handle()),
+               "sp_frames_cplx")
+    return out

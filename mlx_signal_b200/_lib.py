@@ -35,6 +35,14 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
          c_p],
     ),
     "sp_welch_spectral_bins": (c_i, [c_i]),
+    "sp_welch_c64": (
+        c_i,
+        [c_fp, c_i64, c_i64, c_i64, c_fp, c_i, c_i, c_i, c_i, c_fp, c_p, c_sz, c_p],
+    ),
+    "sp_frames_cplx": (
+        c_i,
+        [c_fp, c_i64, c_i64, c_i64, c_i, c_i, c_i64, c_fp, c_i, c_i, c_i, c_i, c_i, c_fp, c_p],
+    ),
     "sp_welch_f32_noalloc": (
         c_i,
         [c_fp, c_i64, c_i64, c_i64, c_fp, c_i, c_i, c_i, c_i, c_i, c_fp, c_p],

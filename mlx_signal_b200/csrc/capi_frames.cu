@@ -107,10 +107,76 @@ int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n
   return SP_OK;
 }
 
+// Per-frame spectra of complex rows (x interleaved complex64, ld in complex elements):
+// power-of-two nfft, two-sided, one frame per transform.
+int run_frames_cplx(const float* x, int64_t rows, int64_t n, int64_t ld, int ext, int ext_mode,
+                    int64_t n_total, const float* win, int nperseg, int nfft, int hop, int detrend,
+                    int power, float* out, void* stream) {
+  if (!x || !win || !out || ld < n) {
+    set_error("null pointer or row stride smaller than n");
+    return SP_ERR_ARG;
+  }
+  if (rows < 0 || n < 1 || ext < 0 || ext_mode < 0 || ext_mode > 4 || n_total < n + 2 * ext ||
+      nperseg < 1 || nperseg > n_total || hop < 1 || hop > nperseg || nfft < nperseg ||
+      detrend < 0 || detrend > 2 || n_total >= (int64_t(1) << 31) ||
+      ((ext_mode == kExtEven || ext_mode == kExtOdd) && ext > n - 1)) {
+    set_error("invalid frame arguments (n=%lld ext=%d n_total=%lld nperseg=%d hop=%d)",
+              (long long)n, ext, (long long)n_total, nperseg, hop);
+    return SP_ERR_ARG;
+  }
+  const int log_l = ilog2_exact(nfft);
+  if (log_l < 0 || log_l > kMaxLogL) {
+    set_error("nfft=%d: complex-input frame kernels need a power of two <= %d", nfft,
+              1 << kMaxLogL);
+    return SP_ERR_UNSUPPORTED;
+  }
+  const FrameInfo f = power ? cplx_lookup_frames_power(log_l, detrend)
+                            : cplx_lookup_frames_stft(log_l, detrend);
+  const int nseg = int((n_total - nperseg) / hop + 1);
+  const int64_t total = rows * nseg;
+  if (total == 0) return SP_OK;
+  int sms = 0;
+  const int nb = resident_ctas(f.fn, f.threads, f.smem, &sms);
+  if (nb <= 0) {
+    set_error("no resident CTA for complex frame kernel (nfft=%d)", nfft);
+    return SP_ERR_UNSUPPORTED;
+  }
+  int64_t blocks = cdiv(total, f.teams);
+  const int64_t cap = int64_t(nb) * sms;
+  if (blocks > cap) blocks = cap;
+  FrameParams p = {};
+  p.x = x;
+  p.ld_x = ld;
+  p.rows = rows;
+  p.n = n;
+  p.ext = ext;
+  p.ext_mode = ext_mode;
+  p.n_ext = n_total;
+  p.nperseg = nperseg;
+  p.hop = hop;
+  p.nseg = nseg;
+  p.detrend = detrend;
+  p.win = win;
+  p.nbins = nfft;
+  p.total = total;
+  p.out = out;
+  p.nfft = nfft;
+  f.launch(dim3(unsigned(blocks)), f.threads, f.smem, static_cast<cudaStream_t>(stream), p);
+  B2S_CHECK_CUDA(cudaGetLastError(), "complex frame kernel launch");
+  return SP_OK;
+}
+
 }  // namespace
 }  // namespace b2s
 
 extern "C" {
+
+int sp_frames_cplx(const float* x, int64_t rows, int64_t n, int64_t ld, int ext, int ext_mode,
+                   int64_t n_total, const float* win, int nperseg, int nfft, int hop, int detrend,
+                   int power, float* out, void* stream) {
+  return b2s::run_frames_cplx(x, rows, n, ld, ext, ext_mode, n_total, win, nperseg, nfft, hop,
+                              detrend, power, out, stream);
+}
 
 int sp_stft_c64(const float* x, int64_t rows, int64_t n, int64_t ld, int ext, int ext_mode,
                 int64_t n_total, const float* win, int nperseg, int nfft, int hop, int detrend,

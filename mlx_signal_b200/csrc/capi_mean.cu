@@ -36,7 +36,12 @@ __global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p)
   const int nsl = int(t1 - t0 + 1);
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   if (live) {
-    if (p.mode == 0) {
+    if (p.mode == 3) {
+      const int stride = cross_q_floats(L);
+      const float* q = p.partial + r * p.cmax * int64_t(stride) + k;
+#pragma unroll 4
+      for (int c = grp; c < nsl; c += kRedGroups) a0 += double(q[int64_t(c) * stride]);
+    } else if (p.mode == 0) {
       const int stride = welch_slot_floats(L);
       const float* q = p.partial + r * p.cmax * int64_t(stride) + kc;
 #pragma unroll 4
@@ -72,6 +77,10 @@ __global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p)
   if (p.onesided && k != 0 && 2 * k != L) fac *= 2.0;
   if (p.mode == 0) {
     p.out[idx] = float(0.5 * a0 * fac);
+    return;
+  }
+  if (p.mode == 3) {  // complex input: two-sided, no mirror
+    p.out[idx] = float(a0 * fac);
     return;
   }
   const double qk = a0, qm = a1, cr = a2, ci = a3;
@@ -114,7 +123,9 @@ int spectral_bins(int log_l) { return (1 << log_l) >> team_log_e_rt(log_l); }
 // coherence, sizes every variant's launch.
 int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop, int detrend,
               MeanPlanInfo* pl, bool spectral = false) {
-  const bool cross = mode != 0;
+  // mode 3: welch of complex rows (one segment per transform, two-sided)
+  const bool cplx = mode == 3;
+  const bool cross = mode == 1 || mode == 2;
   if (rows < 0 || n < 1 || nperseg < 1 || nperseg > n || hop < 1 || hop > nperseg ||
       nfft < nperseg || detrend < 0 || detrend > 2 || n >= (int64_t(1) << 31)) {
     set_error("invalid spectral-mean arguments (rows=%lld n=%lld nperseg=%d nfft=%d hop=%d)",
@@ -123,17 +134,20 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   }
   int log_l = ilog2_exact(nfft);
   // welch with a non-power-of-two nfft: the Bluestein kernel on a power-of-two transform
-  const bool blue = log_l < 0 && !cross && nfft >= 3 && nfft <= kBlueMaxN;
+  const bool blue = log_l < 0 && mode == 0 && nfft >= 3 && nfft <= kBlueMaxN;
   if (!blue && (log_l < 0 || log_l > kMaxLog)) {
     set_error("nfft=%d: fused kernels need a power of two <= %d (welch: or any nfft <= %d)",
               nfft, 1 << kMaxLog, kBlueMaxN);
     return SP_ERR_UNSUPPORTED;
   }
   if (blue) log_l = blue_log_m(nfft);
-  const bool half = !blue && log_l >= 1 && nperseg == nfft && 2 * hop == nperseg && detrend <= 1;
+  const bool half = !blue && !cplx && log_l >= 1 && nperseg == nfft && 2 * hop == nperseg &&
+                    detrend <= 1;
   const int hdet = (spectral && detrend == 1) ? 2 : detrend;  // lookup index: 2 = spectral
   MeanInfo canon;
-  if (blue) {
+  if (cplx) {
+    pl->k = canon = cplx_lookup_welch(log_l, detrend);
+  } else if (blue) {
     pl->k = canon = blue_lookup_welch(log_l, detrend);
   } else if (cross && half) {
     pl->k = mean_lookup_cross_half(log_l, hdet, mode == 1);
@@ -161,14 +175,15 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   }
   const int64_t cap = int64_t(nb) * sms * canon.teams;
   const int64_t total = pl->total > 0 ? pl->total : 1;
-  pl->G = cross ? cdiv(total, cap) : 2 * cdiv(total, 2 * cap);
+  pl->G = (cross || cplx) ? cdiv(total, cap) : 2 * cdiv(total, 2 * cap);
   if (pl->G < 1) pl->G = 1;
   pl->nteams = cdiv(total, pl->G);
   pl->blocks = cdiv(pl->nteams, pl->k.teams);
   int64_t cm = cdiv(pl->nseg, pl->G) + 1;
   if (cm > pl->nteams) cm = pl->nteams;
   pl->cmax = int(cm);
-  pl->slot_floats = cross ? cross_slot_floats(nfft) : welch_slot_floats(nfft);
+  pl->slot_floats = cross ? cross_slot_floats(nfft)
+                          : (cplx ? cross_q_floats(nfft) : welch_slot_floats(nfft));
   pl->ws_bytes = rows * pl->cmax * pl->slot_floats * int64_t(sizeof(float));
   return SP_OK;
 }
@@ -177,7 +192,7 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
              int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
              int onesided, float* out, void* ws, size_t ws_bytes, void* stream,
              const float* wdft = nullptr, int n_low = 0) {
-  const bool cross = mode != 0;
+  const bool cross = mode == 1 || mode == 2;
   if (!x || !win || !out || (cross && !y) || ldx < n || (cross && ldy < n)) {
     set_error("null pointer or row stride smaller than n");
     return SP_ERR_ARG;
@@ -305,7 +320,8 @@ int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld, co
 int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
                                int detrend) {
   b2s::MeanPlanInfo pl;
-  const int st = b2s::make_plan(kind != 0 ? 2 : 0, rows, n, nperseg, nfft, hop, detrend, &pl);
+  const int mode = kind == 3 ? 3 : (kind != 0 ? 2 : 0);
+  const int st = b2s::make_plan(mode, rows, n, nperseg, nfft, hop, detrend, &pl);
   return st == SP_OK ? pl.ws_bytes : int64_t(st);
 }
 
@@ -314,6 +330,13 @@ int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, const floa
                  void* workspace, size_t workspace_bytes, void* stream) {
   return b2s::run_mean(0, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, onesided,
                        out, workspace, workspace_bytes, stream);
+}
+
+int sp_welch_c64(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
+                 int nperseg, int nfft, int hop, int detrend, float* out, void* workspace,
+                 size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(3, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, 0, out,
+                       workspace, workspace_bytes, stream);
 }
 
 int sp_welch_spectral_bins(int nfft) {

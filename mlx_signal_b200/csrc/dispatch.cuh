@@ -7,6 +7,7 @@
 #include <utility>
 
 #include "blue_kernels.cuh"
+#include "cplx_kernels.cuh"
 #include "frame_kernels.cuh"
 #include "istft_kernels.cuh"
 #include "mean_kernels.cuh"
@@ -73,6 +74,10 @@ inline int blue_log_m(int nfft) {
   return lm;
 }
 MeanInfo blue_lookup_welch(int log_m, int det);
+// complex input, power-of-two nfft (log_l in [0, kMaxLogL]); det 0 none, 1 constant, 2 linear
+MeanInfo cplx_lookup_welch(int log_l, int det);
+FrameInfo cplx_lookup_frames_stft(int log_l, int det);
+FrameInfo cplx_lookup_frames_power(int log_l, int det);
 FrameInfo blue_lookup_frames_stft(int log_m, int det);
 FrameInfo blue_lookup_frames_power(int log_m, int det);
 // hop == nperseg/2 == nfft/2, nfft >= 64 (empty info below); det 0/1/2(spectral)

@@ -9,8 +9,9 @@ Routing (the reference's `_stft_metal.eligible` rule, spectral.py:319-347, widen
 float32 input with a power-of-two nfft <= 4096 and detrend in {False, 'constant', 'linear'}
 runs the fused CUDA kernels (segment gather + detrend + window + FFT + |X|^2 or X conj(Y) +
 segment mean in one sweep); welch, stft and spectrogram with any other nfft <= 2048 run fused
-Bluestein (chirp-z) kernels. Other shapes (larger non-power-of-two nfft, non-power-of-two csd /
-coherence of two signals, complex input, median averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
+Bluestein (chirp-z) kernels, and of complex input (power-of-two nfft) the two-sided complex-input
+kernels. Other shapes (larger non-power-of-two nfft, non-power-of-two csd / coherence of two
+signals, csd of two complex signals, median averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
 counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing runs on the CPU.
 """
 
@@ -363,6 +364,8 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
     s.fused = (not x_complex) and (not y_complex) and _kernels.fused_mean_ok(nfft)
     # non-power-of-two nfft: Bluestein kernels for welch / stft / spectrogram (same-input kinds)
     s.blue = (not x_complex) and (not y_complex) and _kernels.blue_ok(nfft)
+    # complex input (same signal), power-of-two nfft: the two-sided complex-input kernels
+    s.cplx = x_complex and same and _kernels.fused_mean_ok(nfft)
     return s
 
 
@@ -509,9 +512,12 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     outer = tuple(X.shape[:-1]) if same else s.outershape
     n = X.shape[-1]
     nseg = (n - s.nperseg) // s.nstep + 1
-    if average == "mean" and (s.fused or (same and s.blue)):
+    if average == "mean" and (s.fused or (same and s.blue) or s.cplx):
         rows = int(np.prod(outer)) if outer else 1
-        if same:
+        if s.cplx:
+            res = _kernels.welch_mean_complex(X.reshape(rows, n), s.win, s.nperseg, s.nfft,
+                                              s.nstep, s.code)
+        elif same:
             res = _kernels.welch_mean(X.reshape(rows, n), s.win, s.nperseg, s.nfft, s.nstep,
                                       s.code, s.onesided, wdft=_spectral_detrend_table(s))
         else:
@@ -653,6 +659,14 @@ def coherence(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=Non
 def _frames_result(s, mode: str) -> torch.Tensor:
     """Per-frame spectra (..., nseg, nfreq): complex (stft) or power (psd)."""
     X = s.X
+    if s.cplx:
+        outer = tuple(X.shape[:-1])
+        rows = int(np.prod(outer)) if outer else 1
+        n = X.shape[-1]
+        res = _kernels.frames_complex("power" if mode == "psd" else "stft", X.reshape(rows, n),
+                                      s.win, s.nperseg, s.nfft, s.nstep, s.code, ext=s.ext,
+                                      ext_mode=s.boundary, n_total=s.n_total)
+        return res.reshape(outer + res.shape[-2:])
     if s.fused or s.blue:
         outer = tuple(X.shape[:-1])
         rows = int(np.prod(outer)) if outer else 1

@@ -400,3 +400,30 @@ def test_bluestein_spectrogram_matches_scipy(rng, mode):
     f, t, s = msig.spectrogram(x, **kw)
     assert tuple(s.shape) == s_ref.shape
     assert_close(s, s_ref, rtol=1e-3 if mode == "phase" else 1e-4)
+
+
+# complex input, power-of-two nfft: fused two-sided complex-input frame kernels
+@pytest.mark.parametrize("kw", [{}, {"nperseg": 1024, "boundary": "even"},
+                                {"nperseg": 128, "noverlap": 96, "boundary": "odd"},
+                                {"nperseg": 256, "boundary": "constant", "detrend": "constant"},
+                                {"nperseg": 64, "nfft": 128, "boundary": None, "padded": False,
+                                 "detrend": "linear"}])
+def test_complex_input_stft_matches_scipy(rng, kw):
+    x = (make_sig(rng, (2, 5001)) + 1j * make_sig(rng, (2, 5001))).astype(np.complex64)
+    x[0] += 1.0 + 1.0j
+    f_ref, t_ref, z_ref = sps.stft(x.astype(np.complex128), **kw)
+    f, t, z = msig.stft(torch.from_numpy(x).cuda(), **kw)
+    assert tuple(z.shape) == z_ref.shape
+    assert_close(f, f_ref)
+    assert_close(t, t_ref)
+    assert_close(z, z_ref)
+
+
+@pytest.mark.parametrize("mode", ["psd", "complex", "magnitude"])
+def test_complex_input_spectrogram_matches_scipy(rng, mode):
+    x = (make_sig(rng, (3, 6000)) + 1j * make_sig(rng, (3, 6000))).astype(np.complex64)
+    kw = dict(nperseg=256, noverlap=64, mode=mode)
+    f_ref, t_ref, s_ref = sps.spectrogram(x.astype(np.complex128), **kw)
+    f, t, s = msig.spectrogram(x, **kw)
+    assert tuple(s.shape) == s_ref.shape
+    assert_close(s, s_ref)

@@ -344,3 +344,26 @@ def test_bluestein_welch_north_star_shape(rng):
     f_ref, p_ref = sps.welch(x.astype(np.float64), fs=48000, nperseg=1000)
     f, p = msig.welch(torch.from_numpy(x).cuda(), fs=48000, nperseg=1000)
     assert rel_err_bins(p, p_ref) <= 1e-5
+
+
+# complex input, power-of-two nfft: fused two-sided complex-input kernel
+@pytest.mark.parametrize("kw", [{}, {"nperseg": 1024}, {"nperseg": 128, "noverlap": 100},
+                                {"nperseg": 64, "nfft": 256, "detrend": "linear"},
+                                {"nperseg": 4096, "detrend": False, "scaling": "spectrum"},
+                                {"nperseg": 1}, {"nperseg": 32, "window": ("tukey", 0.5)}])
+def test_complex_input_welch_matches_scipy(rng, kw):
+    x = (make_sig(rng, (3, 9000)) + 1j * make_sig(rng, (3, 9000))).astype(np.complex64)
+    x[1] += 0.5 - 2j
+    f_ref, p_ref = sps.welch(x.astype(np.complex128), fs=2.0, **kw)
+    f, p = msig.welch(torch.from_numpy(x).cuda(), fs=2.0, **kw)
+    assert tuple(p.shape) == p_ref.shape and p.dtype == torch.float32
+    assert_close(f, f_ref)
+    assert_close(p, p_ref)
+
+
+def test_complex_input_welch_axis_and_rows(rng):
+    x = (make_sig(rng, (4000, 2, 3)) + 1j * make_sig(rng, (4000, 2, 3))).astype(np.complex64)
+    f_ref, p_ref = sps.welch(x.astype(np.complex128), nperseg=256, axis=0)
+    f, p = msig.welch(x, nperseg=256, axis=0)
+    assert tuple(p.shape) == p_ref.shape
+    assert_close(p, p_ref)
