@@ -315,4 +315,86 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_frames(FramePa
   }
 }
 
+// csd / coherence partials for non-power-of-two nfft = pr.nfft, z = x_s + i y_s per segment: the
+// slot layout of k_cross_mean with the N-periodic mirror, Q_k = sum |Z_k|^2 (k < N) and
+// C_k = sum Z_k Z_{N-k} (k <= N/2), Z_k = d_k conj(V_k).
+template <int LOG_M, int DET>
+__global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_cross(MeanParams pr) {
+  using CFG = BlueCfg<LOG_M>;
+  using PL = typename CFG::PL;
+  constexpr int E = PL::E, P = PL::P;
+  const int N = pr.nfft;
+  const BlueSmem sm = blue_smem_setup<CFG>(pr.win, pr.nperseg, N, true);
+  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+  const unsigned mask = team_mask<P>();
+  float4* scratch = sm.scratch + team * CFG::SCRATCH;
+  float2* buf = sm.buf + team * PL::BUF;
+  float2 bh[E];
+  blue_filter<PL>(bh, N, buf, sm.tw, t, mask);
+  const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
+  int64_t g = tau * pr.G;
+  const int64_t gend = min(g + pr.G, pr.total);
+  float q[E];
+  float2 c[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    q[e] = 0.f;
+    c[e] = make_float2(0.f, 0.f);
+  }
+  while (g < gend) {
+    const int64_t r = g / pr.nseg;
+    const int s0 = int(g - r * pr.nseg);
+    const int64_t lim = int64_t(s0) + (gend - g);
+    const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
+    const float* xr = pr.x + r * pr.ld_x;
+    const float* yr = pr.y + r * pr.ld_y;
+    for (int s = s0; s < s1; ++s) {
+      const float* xs = xr + int64_t(s) * pr.hop;
+      const float* ys = yr + int64_t(s) * pr.hop;
+      float2 v[E];
+      static_for<0, E>([&](auto ec) {
+        constexpr int e = decltype(ec)::value;
+        const int n = slot_elem<PL, e>(t);
+        const bool ok = n < pr.nperseg;
+        v[e].x = ok ? __ldg(xs + n) : 0.f;
+        v[e].y = ok ? __ldg(ys + n) : 0.f;
+      });
+      blue_premultiply<PL, DET>(v, sm.cin, pr.nperseg, t, scratch, mask);
+      blue_core<PL>(v, bh, buf, sm.tw, t, mask);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = t + e * P;
+        if (k < N) {
+          q[e] = fmaf(v[e].x, v[e].x, fmaf(v[e].y, v[e].y, q[e]));
+          v[e] = cmul(sm.cout[k], make_float2(v[e].x, -v[e].y));
+          buf[PL::pad(k)] = v[e];
+        }
+      }
+      team_sync<P>(mask);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = t + e * P;
+        if (2 * k <= N) {
+          const float2 m = buf[PL::pad(k == 0 ? 0 : N - k)];
+          c[e].x = fmaf(v[e].x, m.x, fmaf(-v[e].y, m.y, c[e].x));
+          c[e].y = fmaf(v[e].x, m.y, fmaf(v[e].y, m.x, c[e].y));
+        }
+      }
+      team_sync<P>(mask);
+    }
+    const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
+    float* dst = pr.partial + (r * pr.cmax + slot) * int64_t(cross_slot_floats(N));
+    float2* dstc = reinterpret_cast<float2*>(dst + cross_q_floats(N));
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = t + e * P;
+      if (k < N) dst[k] = q[e];
+      if (2 * k <= N) dstc[k] = c[e];
+      q[e] = 0.f;
+      c[e] = make_float2(0.f, 0.f);
+    }
+    g += s1 - s0;
+  }
+}
+
 }  // namespace b2s

@@ -134,9 +134,9 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   }
   int log_l = ilog2_exact(nfft);
   // welch with a non-power-of-two nfft: the Bluestein kernel on a power-of-two transform
-  const bool blue = log_l < 0 && mode == 0 && nfft >= 3 && nfft <= kBlueMaxN;
+  const bool blue = log_l < 0 && !cplx && nfft >= 3 && nfft <= kBlueMaxN;
   if (!blue && (log_l < 0 || log_l > kMaxLog)) {
-    set_error("nfft=%d: fused kernels need a power of two <= %d (welch: or any nfft <= %d)",
+    set_error("nfft=%d: fused kernels need a power of two <= %d (or any nfft <= %d)",
               nfft, 1 << kMaxLog, kBlueMaxN);
     return SP_ERR_UNSUPPORTED;
   }
@@ -148,7 +148,7 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   if (cplx) {
     pl->k = canon = cplx_lookup_welch(log_l, detrend);
   } else if (blue) {
-    pl->k = canon = blue_lookup_welch(log_l, detrend);
+    pl->k = canon = cross ? blue_lookup_cross(log_l, detrend) : blue_lookup_welch(log_l, detrend);
   } else if (cross && half) {
     pl->k = mean_lookup_cross_half(log_l, hdet, mode == 1);
     canon = mean_lookup_cross_half(log_l, detrend, false);

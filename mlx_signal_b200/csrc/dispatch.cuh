@@ -74,6 +74,7 @@ inline int blue_log_m(int nfft) {
   return lm;
 }
 MeanInfo blue_lookup_welch(int log_m, int det);
+MeanInfo blue_lookup_cross(int log_m, int det);  // csd / coherence (same slots as k_cross_mean)
 // complex input, power-of-two nfft (log_l in [0, kMaxLogL]); det 0 none, 1 constant, 2 linear
 MeanInfo cplx_lookup_welch(int log_l, int det);
 FrameInfo cplx_lookup_frames_stft(int log_l, int det);

@@ -8,10 +8,10 @@ complex64). Computation is float32/complex64.
 Routing (the reference's `_stft_metal.eligible` rule, spectral.py:319-347, widened): real
 float32 input with a power-of-two nfft <= 4096 and detrend in {False, 'constant', 'linear'}
 runs the fused CUDA kernels (segment gather + detrend + window + FFT + |X|^2 or X conj(Y) +
-segment mean in one sweep); welch, stft and spectrogram with any other nfft <= 2048 run fused
-Bluestein (chirp-z) kernels, and of complex input (power-of-two nfft) the two-sided complex-input
-kernels. Other shapes (larger non-power-of-two nfft, non-power-of-two csd / coherence of two
-signals, csd of two complex signals, median averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
+segment mean in one sweep); any other nfft <= 2048 runs fused Bluestein (chirp-z) kernels, and
+welch / stft / spectrogram of complex input (power-of-two nfft) the two-sided complex-input
+kernels. Other shapes (larger non-power-of-two nfft, csd of two complex signals, median
+averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
 counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing runs on the CPU.
 """
 
@@ -362,7 +362,7 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
     s.win = device_vector((win_np * np.sqrt(scale)).astype(np.float32))
     s.freqs = _freqs(nfft, fs, onesided)
     s.fused = (not x_complex) and (not y_complex) and _kernels.fused_mean_ok(nfft)
-    # non-power-of-two nfft: Bluestein kernels for welch / stft / spectrogram (same-input kinds)
+    # non-power-of-two nfft <= 2048: Bluestein (chirp-z) kernels
     s.blue = (not x_complex) and (not y_complex) and _kernels.blue_ok(nfft)
     # complex input (same signal), power-of-two nfft: the two-sided complex-input kernels
     s.cplx = x_complex and same and _kernels.fused_mean_ok(nfft)
@@ -512,7 +512,7 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     outer = tuple(X.shape[:-1]) if same else s.outershape
     n = X.shape[-1]
     nseg = (n - s.nperseg) // s.nstep + 1
-    if average == "mean" and (s.fused or (same and s.blue) or s.cplx):
+    if average == "mean" and (s.fused or s.blue or s.cplx):
         rows = int(np.prod(outer)) if outer else 1
         if s.cplx:
             res = _kernels.welch_mean_complex(X.reshape(rows, n), s.win, s.nperseg, s.nfft,
@@ -616,7 +616,8 @@ def coherence(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=Non
               detrend="constant", axis=-1):
     """Magnitude-squared coherence |Pxy|^2/(Pxx Pyy) (scipy.signal.coherence semantics).
 
-    Fast path (equal-shape real inputs, power-of-two nfft): one fused sweep computes Pxx, Pyy
+    Fast path (equal-shape real inputs; a power-of-two nfft, or any nfft <= 2048 through the
+    chirp-z kernels): one fused sweep computes Pxx, Pyy
     and Pxy together; scale factors cancel so the raw window is used (reference
     spectral.py:591-617). The ratio is guarded (0 where Pxx*Pyy == 0) and clamped to [0, 1].
     """
@@ -626,7 +627,7 @@ def coherence(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=Non
         win_np, nps = _triage_segments(window, nperseg, input_length=X.shape[axis])
         nov = nps // 2 if noverlap is None else int(noverlap)
         nft = nps if nfft is None else int(nfft)
-        if nov < nps and nft >= nps and _kernels.fused_mean_ok(nft):
+        if nov < nps and nft >= nps and (_kernels.fused_mean_ok(nft) or _kernels.blue_ok(nft)):
             code = _detrend_code(detrend)
             ax = axis % X.dim()
             if X.dim() > 1 and ax != X.dim() - 1:

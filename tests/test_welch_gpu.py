@@ -367,3 +367,20 @@ def test_complex_input_welch_axis_and_rows(rng):
     f, p = msig.welch(x, nperseg=256, axis=0)
     assert tuple(p.shape) == p_ref.shape
     assert_close(p, p_ref)
+
+
+@pytest.mark.parametrize("kw", [{"nperseg": 1000}, {"nperseg": 300, "noverlap": 250},
+                                {"nperseg": 77, "nfft": 99, "detrend": "linear"},
+                                {"nperseg": 1500, "detrend": False, "scaling": "spectrum"}])
+def test_bluestein_csd_coherence_match_scipy(rng, kw):
+    x = make_sig(rng, (2, 30000))
+    y = (0.6 * np.roll(x, 5, axis=-1) + 0.4 * make_sig(rng, (2, 30000))).astype(np.float32)
+    f_ref, c_ref = sps.csd(x.astype(np.float64), y.astype(np.float64), **kw)
+    f, c = msig.csd(x, y, **kw)
+    assert tuple(c.shape) == c_ref.shape
+    assert_close(c, c_ref, rtol=2e-4)
+    kc = {k: v for k, v in kw.items() if k != "scaling"}
+    f_ref, h_ref = sps.coherence(x.astype(np.float64), y.astype(np.float64), **kc)
+    f, h = msig.coherence(x, y, **kc)
+    assert tuple(h.shape) == h_ref.shape
+    assert_close(h, h_ref, rtol=1e-3)
