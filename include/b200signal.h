@@ -166,6 +166,17 @@ SP_API int sp_frames_cplx(const float* x, int64_t rows, int64_t n, int64_t ld, i
                           int ext_mode, int64_t n_total, const float* win, int nperseg, int nfft,
                           int hop, int detrend, int power, float* out, void* stream);
 
+/*
+ * Column medians over segments (average='median'): out[r * ncols + c] = scale * median over
+ * s < nseg of in[(r * nseg + s) * ld_frame + c] (mean of the two middle values for an even nseg),
+ * for per-frame spectra (rows, nseg, ncols) with frame stride ld_frame floats; a complex spectrum
+ * is passed as its float view (real and imaginary parts are separate columns). nseg up to 49151
+ * (staged in shared memory), else SP_ERR_UNSUPPORTED. Replaces the median branch of spectral.csd
+ * (spectral.py:469-477: median of the per-segment spectra along the segment axis / median bias).
+ */
+SP_API int sp_median_frames_f32(const float* in, int64_t rows, int nseg, int ncols,
+                                int64_t ld_frame, float scale, float* out, void* stream);
+
 /* Boundary extension modes of the per-frame entry points (scipy stft `boundary`). */
 enum { SP_EXT_NONE = 0, SP_EXT_ZEROS = 1, SP_EXT_EVEN = 2, SP_EXT_ODD = 3, SP_EXT_CONSTANT = 4 };
 

@@ -306,3 +306,28 @@ def frames_complex(kind: str, x: torch.Tensor, win: torch.Tensor, nperseg: int, 
                                           int(power), out.data_ptr(), stream_handle()),
                "sp_frames_cplx")
     return out
+
+
+def median_segments(per: torch.Tensor, scale: float) -> torch.Tensor | None:
+    """Median over the segment axis of per-frame spectra per (..., nseg, nfreq) (float32, or
+    complex64: real and imaginary parts separately), times `scale` -> (..., nfreq); None when
+    nseg exceeds the kernel's staged maximum (the caller sorts instead)."""
+    cplx = per.is_complex()
+    lead = tuple(per.shape[:-2])
+    nseg, nf = per.shape[-2], per.shape[-1]
+    p = torch.view_as_real(per).flatten(-2) if cplx else per
+    rows = int(np.prod(lead)) if lead else 1
+    ncols = p.shape[-1]
+    p = p.reshape(rows, nseg, ncols)
+    # the kernel reads frame s of row r at (r * nseg + s) * stride(1)
+    if p.stride(2) != 1 or p.stride(1) < ncols or (rows > 1 and p.stride(0) != nseg * p.stride(1)):
+        p = p.contiguous()
+    out = torch.empty((rows, ncols), dtype=torch.float32, device=per.device)
+    st = _lib.load().sp_median_frames_f32(p.data_ptr(), rows, nseg, ncols, p.stride(1),
+                                          float(scale), out.data_ptr(), stream_handle())
+    if st == _lib.SP_ERR_UNSUPPORTED:
+        return None
+    _lib.check(st, "sp_median_frames_f32")
+    if cplx:
+        out = torch.view_as_complex(out.reshape(rows, nf, 2))
+    return out.reshape(lead + (nf,))

@@ -99,6 +99,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "sp_conv_ols_f32": (c_i, [c_fp, c_i64, c_i64, c_i64, c_fp, c_i, c_i64, c_i64, c_fp, c_i64,
                               c_p]),
     "sp_conv_block_len": (c_i, [c_i]),
+    "sp_median_frames_f32": (c_i, [c_fp, c_i64, c_i, c_i, c_i64, ctypes.c_float, c_fp, c_p]),
     "sp_batch_stream_frames": (c_i64, [c_i64, c_i64, c_i, c_i, ctypes.POINTER(c_i64)]),
     "sp_batch_supported": (c_i, [c_i]),
     "sp_batch_plan": (c_i, [c_p, c_i, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)]),

@@ -530,13 +530,15 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
             _remember_plan(key, _WelchPlan(s, rows, n, outer))
     else:
         rows = int(np.prod(outer)) if outer else 1
+        folded = False  # per-frame powers already carry the one-sided factor
         if s.fused:
-            # median averaging: per-frame fused kernels, then the order statistic
+            # median averaging: per-frame fused kernels, then the order statistic. The power
+            # frames come one-sided with the factor 2 applied (it commutes with the median).
             if same:
                 per = _kernels.frames("power", X.reshape(rows, n), s.win, s.nperseg, s.nfft,
-                                      s.nstep, s.code, False)
-                if s.onesided:
-                    per = per[..., : s.nfft // 2 + 1]
+                                      s.nstep, s.code, s.onesided,
+                                      wdft=_spectral_detrend_table(s, frames=True))
+                folded = s.onesided
             else:
                 Xb = X.expand(outer + (n,)).reshape(rows, n)
                 Yb = Y.expand(outer + (n,)).reshape(rows, n)
@@ -551,8 +553,14 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
             else:
                 fy = _composed_spectra(Y, s.win, s.code, s.nperseg, s.nstep, s.nfft, s.onesided)
                 per = torch.conj(fx) * fy
+        med = None
+        if nseg > 1 and average == "median":
+            # column-median kernel over the (..., nseg, nfreq) frames; median bias folded in
+            med = _kernels.median_segments(per, 1.0 / _median_bias(nseg))
         per = per.movedim(-2, -1)  # (..., nfreq, nseg)
-        if nseg > 1:
+        if med is not None:
+            pxy = med
+        elif nseg > 1:
             if average == "median":
                 bias = _median_bias(nseg)
                 if per.is_complex():
@@ -564,7 +572,7 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
                 pxy = per.mean(dim=-1)
         else:
             pxy = per[..., 0]
-        if s.onesided:
+        if s.onesided and not folded:
             pxy = pxy * device_vector(_onesided_factor_np(s.nfft))
     if pxy.dim() > 1 and s.axis != -1:
         pxy = pxy.movedim(-1, s.axis if s.axis >= 0 else pxy.dim() + s.axis)

@@ -384,3 +384,31 @@ def test_bluestein_csd_coherence_match_scipy(rng, kw):
     f, h = msig.coherence(x, y, **kc)
     assert tuple(h.shape) == h_ref.shape
     assert_close(h, h_ref, rtol=1e-3)
+
+
+# average='median': column-median kernel over the per-frame spectra
+@pytest.mark.parametrize("n,kw", [(20000, {"nperseg": 128}), (20000, {"nperseg": 256}),
+                                  (4096, {"nperseg": 512, "noverlap": 0}),
+                                  (3000, {"nperseg": 1000}), (9000, {"nperseg": 64,
+                                                                     "detrend": "linear"})])
+def test_median_welch_csd_match_scipy(rng, n, kw):
+    x = make_sig(rng, (3, n))
+    y = (0.5 * x + 0.5 * make_sig(rng, (3, n))).astype(np.float32)
+    f_ref, p_ref = sps.welch(x.astype(np.float64), average="median", **kw)
+    f, p = msig.welch(x, average="median", **kw)
+    assert tuple(p.shape) == p_ref.shape
+    assert_close(p, p_ref)
+    f_ref, c_ref = sps.csd(x.astype(np.float64), y.astype(np.float64), average="median", **kw)
+    f, c = msig.csd(x, y, average="median", **kw)
+    assert_close(c, c_ref, rtol=2e-4)
+
+
+def test_median_ties_and_even_counts(rng):
+    """Repeated values (zero signal, constant rows) and even / odd segment counts."""
+    x = np.zeros((2, 1024 * 9), np.float32)
+    x[1] = 1.0
+    for nperseg in (1024, 2048):  # 17 and 8 segments
+        f_ref, p_ref = sps.welch(x.astype(np.float64), nperseg=nperseg, average="median",
+                                 detrend=False)
+        f, p = msig.welch(x, nperseg=nperseg, average="median", detrend=False)
+        assert_close(p, p_ref)
