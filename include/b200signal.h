@@ -52,8 +52,9 @@ SP_API int sp_version(void);
 SP_API const char* sp_last_error(void);
 
 /*
- * Workspace bytes for sp_welch_f32 (kind 0), sp_csd_c64 / sp_coherence_f32 (kind 1) or
- * sp_welch_c64 (kind 3) on the current device. Negative return = error status.
+ * Workspace bytes for sp_welch_f32 (kind 0), sp_csd_c64 / sp_coherence_f32 (kind 1),
+ * sp_welch_c64 (kind 3) or sp_csd_cplx (kind 4) on the current device. Negative return = error
+ * status.
  * Replaces the implicit group-partial buffers of _stft_metal.rfft_power_mean
  * (_stft_metal.py:530-557) and _pair_sum_launch (_stft_metal.py:703-736).
  */
@@ -83,6 +84,16 @@ SP_API int sp_welch_f32(const float* x, int64_t rows, int64_t n, int64_t ld, con
 SP_API int sp_welch_c64(const float* x, int64_t rows, int64_t n, int64_t ld, const float* win,
                         int nperseg, int nfft, int hop, int detrend, float* out, void* workspace,
                         size_t workspace_bytes, void* stream);
+
+/*
+ * Cross spectral density of complex rows x, y (interleaved complex64, ld in complex elements),
+ * two-sided: out[r][k] = 1/nseg * sum_s conj(X_rs[k]) Y_rs[k] (complex64), k < nfft, nfft a power
+ * of two in [1, 4096]. Workspace: sp_mean_workspace_size(4, ...). Replaces the composed complex
+ * path of spectral.csd (spectral.py:290-298, :127-147: frames + mx.fft.fft of x and y).
+ */
+SP_API int sp_csd_cplx(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+                       int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
+                       float* out, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * sp_welch_f32 with the constant detrend applied in the frequency domain. `win_dft_low` is a

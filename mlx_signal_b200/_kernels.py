@@ -331,3 +331,22 @@ def median_segments(per: torch.Tensor, scale: float) -> torch.Tensor | None:
     if cplx:
         out = torch.view_as_complex(out.reshape(rows, nf, 2))
     return out.reshape(lead + (nf,))
+
+
+def csd_complex(x: torch.Tensor, y: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int,
+                hop: int, detrend: int) -> torch.Tensor:
+    """Two-sided mean conj(X) Y over the segments of complex rows x, y -> (rows, nfft) complex64
+    (power-of-two nfft)."""
+    x, ldx = _rows_c(x)
+    y, ldy = _rows_c(y)
+    rows, n = x.shape
+    lib = _lib.load()
+    ws_bytes = lib.sp_mean_workspace_size(4, rows, n, nperseg, nfft, hop, detrend)
+    if ws_bytes < 0:
+        _lib.check(int(ws_bytes), "sp_mean_workspace_size")
+    out = torch.empty((rows, nfft), dtype=torch.complex64, device=x.device)
+    ws = _workspace(ws_bytes, x.device)
+    _lib.check(lib.sp_csd_cplx(x.data_ptr(), y.data_ptr(), rows, n, ldx, ldy, win.data_ptr(),
+                               nperseg, nfft, hop, detrend, out.data_ptr(), ws.data_ptr(),
+                               ws.numel(), stream_handle()), "sp_csd_cplx")
+    return out

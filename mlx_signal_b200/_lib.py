@@ -39,6 +39,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         c_i,
         [c_fp, c_i64, c_i64, c_i64, c_fp, c_i, c_i, c_i, c_i, c_fp, c_p, c_sz, c_p],
     ),
+    "sp_csd_cplx": (
+        c_i,
+        [c_fp, c_fp, c_i64, c_i64, c_i64, c_i64, c_fp, c_i, c_i, c_i, c_i, c_fp, c_p, c_sz, c_p],
+    ),
     "sp_frames_cplx": (
         c_i,
         [c_fp, c_i64, c_i64, c_i64, c_i, c_i, c_i64, c_fp, c_i, c_i, c_i, c_i, c_i, c_fp, c_p],

@@ -36,7 +36,15 @@ __global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p)
   const int nsl = int(t1 - t0 + 1);
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   if (live) {
-    if (p.mode == 3) {
+    if (p.mode == 4) {
+      const int stride = 2 * L;
+      const float* q = p.partial + r * p.cmax * int64_t(stride) + 2 * k;
+#pragma unroll 2
+      for (int c = grp; c < nsl; c += kRedGroups) {
+        a0 += double(q[int64_t(c) * stride]);
+        a1 += double(q[int64_t(c) * stride + 1]);
+      }
+    } else if (p.mode == 3) {
       const int stride = cross_q_floats(L);
       const float* q = p.partial + r * p.cmax * int64_t(stride) + k;
 #pragma unroll 4
@@ -83,6 +91,11 @@ __global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p)
     p.out[idx] = float(a0 * fac);
     return;
   }
+  if (p.mode == 4) {  // csd of complex inputs: mean conj(X) Y, two-sided
+    p.out[2 * idx] = float(a0 * fac);
+    p.out[2 * idx + 1] = float(a1 * fac);
+    return;
+  }
   const double qk = a0, qm = a1, cr = a2, ci = a3;
   const double pxy_re = 0.5 * ci, pxy_im = 0.25 * (qm - qk);
   if (p.mode == 1) {
@@ -123,8 +136,9 @@ int spectral_bins(int log_l) { return (1 << log_l) >> team_log_e_rt(log_l); }
 // coherence, sizes every variant's launch.
 int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop, int detrend,
               MeanPlanInfo* pl, bool spectral = false) {
-  // mode 3: welch of complex rows (one segment per transform, two-sided)
-  const bool cplx = mode == 3;
+  // mode 3: welch of complex rows (one segment per transform, two-sided); mode 4: csd of two
+  // complex signals (two transforms per segment, two-sided)
+  const bool cplx = mode == 3 || mode == 4;
   const bool cross = mode == 1 || mode == 2;
   if (rows < 0 || n < 1 || nperseg < 1 || nperseg > n || hop < 1 || hop > nperseg ||
       nfft < nperseg || detrend < 0 || detrend > 2 || n >= (int64_t(1) << 31)) {
@@ -146,7 +160,7 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   const int hdet = (spectral && detrend == 1) ? 2 : detrend;  // lookup index: 2 = spectral
   MeanInfo canon;
   if (cplx) {
-    pl->k = canon = cplx_lookup_welch(log_l, detrend);
+    pl->k = canon = mode == 4 ? cplx_lookup_csd(log_l, detrend) : cplx_lookup_welch(log_l, detrend);
   } else if (blue) {
     pl->k = canon = cross ? blue_lookup_cross(log_l, detrend) : blue_lookup_welch(log_l, detrend);
   } else if (cross && half) {
@@ -183,7 +197,8 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   if (cm > pl->nteams) cm = pl->nteams;
   pl->cmax = int(cm);
   pl->slot_floats = cross ? cross_slot_floats(nfft)
-                          : (cplx ? cross_q_floats(nfft) : welch_slot_floats(nfft));
+                          : (mode == 4 ? 2 * int64_t(nfft)
+                                       : (cplx ? cross_q_floats(nfft) : welch_slot_floats(nfft)));
   pl->ws_bytes = rows * pl->cmax * pl->slot_floats * int64_t(sizeof(float));
   return SP_OK;
 }
@@ -192,7 +207,7 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
              int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
              int onesided, float* out, void* ws, size_t ws_bytes, void* stream,
              const float* wdft = nullptr, int n_low = 0) {
-  const bool cross = mode == 1 || mode == 2;
+  const bool cross = mode == 1 || mode == 2 || mode == 4;  // two input signals
   if (!x || !win || !out || (cross && !y) || ldx < n || (cross && ldy < n)) {
     set_error("null pointer or row stride smaller than n");
     return SP_ERR_ARG;
@@ -320,7 +335,7 @@ int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld, co
 int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
                                int detrend) {
   b2s::MeanPlanInfo pl;
-  const int mode = kind == 3 ? 3 : (kind != 0 ? 2 : 0);
+  const int mode = (kind == 3 || kind == 4) ? kind : (kind != 0 ? 2 : 0);
   const int st = b2s::make_plan(mode, rows, n, nperseg, nfft, hop, detrend, &pl);
   return st == SP_OK ? pl.ws_bytes : int64_t(st);
 }
@@ -336,6 +351,13 @@ int sp_welch_c64(const float* x, int64_t rows, int64_t n, int64_t ld, const floa
                  int nperseg, int nfft, int hop, int detrend, float* out, void* workspace,
                  size_t workspace_bytes, void* stream) {
   return b2s::run_mean(3, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, 0, out,
+                       workspace, workspace_bytes, stream);
+}
+
+int sp_csd_cplx(const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
+                int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
+                float* out, void* workspace, size_t workspace_bytes, void* stream) {
+  return b2s::run_mean(4, x, y, rows, n, ldx, ldy, win, nperseg, nfft, hop, detrend, 0, out,
                        workspace, workspace_bytes, stream);
 }
 

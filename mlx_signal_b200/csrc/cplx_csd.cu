@@ -1,0 +1,27 @@
+// Instantiations of k_csd_cplx (csd of complex input) for every fused nfft and detrend kind.
+#include "dispatch.cuh"
+
+namespace b2s {
+namespace {
+template <int LOG_L, int DET>
+struct F {
+  static void launch(dim3 g, int t, size_t sm, cudaStream_t st, const MeanParams& p) {
+    k_csd_cplx<LOG_L, team_log_e<LOG_L>(), DET><<<g, t, sm, st>>>(p);
+  }
+  static MeanInfo get() {
+    using CFG = MeanCfg<LOG_L, team_log_e<LOG_L>()>;
+    MeanInfo k;
+    k.fn = reinterpret_cast<const void*>(&k_csd_cplx<LOG_L, team_log_e<LOG_L>(), DET>);
+    k.threads = CFG::THREADS;
+    // exchange buffers plus one parked transform (L complex) per team
+    k.smem = CFG::SMEM + size_t(CFG::TEAMS) * CFG::PL::L * 8;
+    k.teams = CFG::TEAMS;
+    k.launch = &launch;
+    return k;
+  }
+};
+}  // namespace
+
+MeanInfo cplx_lookup_csd(int log_l, int det) { return lookup_all<MeanInfo, F>(log_l, det); }
+
+}  // namespace b2s

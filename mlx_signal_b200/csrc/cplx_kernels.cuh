@@ -149,4 +149,67 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   }
 }
 
+// csd of complex rows x, y (interleaved complex64, ld in complex elements): partial[r][slot][k] =
+// sum over the team's segments of conj(X_k) Y_k, k in [0, L) (slot stride 2L floats). Each
+// segment is two team transforms; X is parked in shared memory in the thread's own bins.
+template <int LOG_L, int LOG_E, int DET>
+__global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
+    k_csd_cplx(MeanParams pr) {
+  using CFG = MeanCfg<LOG_L, LOG_E>;
+  using PL = typename CFG::PL;
+  constexpr int L = PL::L, E = PL::E, P = PL::P;
+  const MeanSmem sm = mean_smem_setup<CFG>(pr.win, pr.nperseg);
+  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+  const unsigned mask = team_mask<P>();
+  float4* scratch = sm.scratch + team * CFG::SCRATCH;
+  float2* buf = sm.buf + team * PL::BUF;
+  // per-team parking area for X after the exchange buffers
+  float2* xs_park = sm.buf + CFG::TEAMS * PL::BUF + team * L;
+  const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
+  int64_t g = tau * pr.G;
+  const int64_t gend = min(g + pr.G, pr.total);
+  const float2* x = reinterpret_cast<const float2*>(pr.x);
+  const float2* y = reinterpret_cast<const float2*>(pr.y);
+  float2 acc[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) acc[e] = make_float2(0.f, 0.f);
+  auto transform = [&](const float2* seg, float2 (&v)[E]) {
+    static_for<0, E>([&](auto ec) {
+      constexpr int e = decltype(ec)::value;
+      const int n = slot_elem<PL, e>(t);
+      v[e] = n < pr.nperseg ? __ldg(seg + n) : make_float2(0.f, 0.f);
+    });
+    detrend_window<PL, DET>(v, sm.win, t, pr.nperseg, scratch, mask);
+    team_pass0<PL>(v);
+    team_passes<PL>(v, buf, sm.tw, t, mask);
+  };
+  while (g < gend) {
+    const int64_t r = g / pr.nseg;
+    const int s0 = int(g - r * pr.nseg);
+    const int64_t lim = int64_t(s0) + (gend - g);
+    const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
+    for (int s = s0; s < s1; ++s) {
+      float2 v[E];
+      transform(x + r * pr.ld_x + int64_t(s) * pr.hop, v);
+#pragma unroll
+      for (int e = 0; e < E; ++e) xs_park[t + e * P] = v[e];
+      transform(y + r * pr.ld_y + int64_t(s) * pr.hop, v);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const float2 a = xs_park[t + e * P];  // X_k; accumulate conj(X_k) Y_k
+        acc[e].x = fmaf(a.x, v[e].x, fmaf(a.y, v[e].y, acc[e].x));
+        acc[e].y = fmaf(a.x, v[e].y, fmaf(-a.y, v[e].x, acc[e].y));
+      }
+    }
+    const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
+    float2* dst = reinterpret_cast<float2*>(pr.partial + (r * pr.cmax + slot) * int64_t(2 * L));
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      dst[t + e * P] = acc[e];
+      acc[e] = make_float2(0.f, 0.f);
+    }
+    g += s1 - s0;
+  }
+}
+
 }  // namespace b2s

@@ -79,6 +79,7 @@ MeanInfo blue_lookup_cross(int log_m, int det);  // csd / coherence (same slots 
 MeanInfo cplx_lookup_welch(int log_l, int det);
 FrameInfo cplx_lookup_frames_stft(int log_l, int det);
 FrameInfo cplx_lookup_frames_power(int log_l, int det);
+MeanInfo cplx_lookup_csd(int log_l, int det);  // csd of two complex signals
 FrameInfo blue_lookup_frames_stft(int log_m, int det);
 FrameInfo blue_lookup_frames_power(int log_m, int det);
 // hop == nperseg/2 == nfft/2, nfft >= 64 (empty info below); det 0/1/2(spectral)

@@ -10,9 +10,11 @@ float32 input with a power-of-two nfft <= 4096 and detrend in {False, 'constant'
 runs the fused CUDA kernels (segment gather + detrend + window + FFT + |X|^2 or X conj(Y) +
 segment mean in one sweep); any other nfft <= 2048 runs fused Bluestein (chirp-z) kernels, and
 welch / stft / spectrogram of complex input (power-of-two nfft) the two-sided complex-input
-kernels. Other shapes (larger non-power-of-two nfft, csd of two complex signals, median
-averaging) run the composed GPU path: strided frames, torch elementwise ops and cuFFT -- the
-counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing runs on the CPU.
+kernels (csd of two signals either of which is complex: the complex cross kernel), median
+averaging the per-frame kernels plus a column-median kernel. Other shapes (larger
+non-power-of-two nfft) run the composed GPU path: strided frames, torch elementwise ops and
+cuFFT -- the counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing runs
+on the CPU.
 """
 
 from __future__ import annotations
@@ -366,6 +368,8 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
     s.blue = (not x_complex) and (not y_complex) and _kernels.blue_ok(nfft)
     # complex input (same signal), power-of-two nfft: the two-sided complex-input kernels
     s.cplx = x_complex and same and _kernels.fused_mean_ok(nfft)
+    # csd of two signals, either complex, power-of-two nfft: the complex cross kernel
+    s.cplx2 = (not same) and (x_complex or y_complex) and _kernels.fused_mean_ok(nfft)
     return s
 
 
@@ -512,9 +516,13 @@ def csd(x, y, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
     outer = tuple(X.shape[:-1]) if same else s.outershape
     n = X.shape[-1]
     nseg = (n - s.nperseg) // s.nstep + 1
-    if average == "mean" and (s.fused or s.blue or s.cplx):
+    if average == "mean" and (s.fused or s.blue or s.cplx or s.cplx2):
         rows = int(np.prod(outer)) if outer else 1
-        if s.cplx:
+        if s.cplx2:
+            Xb = X.to(torch.complex64).expand(outer + (n,)).reshape(rows, n)
+            Yb = Y.to(torch.complex64).expand(outer + (n,)).reshape(rows, n)
+            res = _kernels.csd_complex(Xb, Yb, s.win, s.nperseg, s.nfft, s.nstep, s.code)
+        elif s.cplx:
             res = _kernels.welch_mean_complex(X.reshape(rows, n), s.win, s.nperseg, s.nfft,
                                               s.nstep, s.code)
         elif same:

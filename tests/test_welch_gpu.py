@@ -412,3 +412,22 @@ def test_median_ties_and_even_counts(rng):
                                  detrend=False)
         f, p = msig.welch(x, nperseg=nperseg, average="median", detrend=False)
         assert_close(p, p_ref)
+
+
+@pytest.mark.parametrize("kw", [{"nperseg": 256}, {"nperseg": 1024, "detrend": "linear"},
+                                {"nperseg": 64, "nfft": 128, "noverlap": 16}])
+def test_complex_csd_and_coherence_match_scipy(rng, kw):
+    x = (make_sig(rng, (2, 12000)) + 1j * make_sig(rng, (2, 12000))).astype(np.complex64)
+    y = (0.5 * np.roll(x, 3, axis=-1) + 0.5 * make_sig(rng, (2, 12000))).astype(np.complex64)
+    f_ref, c_ref = sps.csd(x.astype(np.complex128), y.astype(np.complex128), **kw)
+    f, c = msig.csd(x, y, **kw)
+    assert tuple(c.shape) == c_ref.shape and c.dtype == torch.complex64
+    assert_close(f, f_ref)
+    assert_close(c, c_ref, rtol=2e-4)
+    xr = make_sig(rng, (2, 12000))  # real x with complex y (scipy wants the two-sided request)
+    f_ref, c_ref = sps.csd(xr.astype(np.float64), y.astype(np.complex128),
+                           return_onesided=False, **kw)
+    assert_close(msig.csd(xr, y, return_onesided=False, **kw)[1], c_ref, rtol=2e-4)
+    f_ref, h_ref = sps.coherence(x.astype(np.complex128), y.astype(np.complex128), **kw)
+    f, h = msig.coherence(x, y, **kw)
+    assert_close(h, h_ref, rtol=1e-3)
