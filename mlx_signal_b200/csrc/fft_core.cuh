@@ -252,16 +252,28 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
   static_for<0, PL::NPASS - 1>([&](auto pc) {
     constexpr int p = decltype(pc)::value;  // pass whose outputs are being stored
     constexpr int R = PL::radix(p), S = PL::span(p), B = PL::E / R;
-    // store pass-p outputs in Stockham order
+    // store pass-p outputs in Stockham order. The padded index pad(base + r S) is pad(base)
+    // plus a compile-time offset whenever adding r S cannot carry into the padding shift: S a
+    // multiple of 2^PADSH, or the R S-aligned block holding base inside one 2^PADSH block.
+    constexpr int PB = 1 << PL::PADSH;
     static_for<0, B>([&](auto bc) {
       constexpr int b = decltype(bc)::value;
       const int j = t + P * b;
       const int jm = j % S;
       const int base = (j - jm) * R + jm;
-      static_for<0, R>([&](auto rc) {
-        constexpr int r = decltype(rc)::value;
-        buf[PL::pad(base + r * S)] = v[b * R + r];
-      });
+      if constexpr (S % PB == 0 || R * S <= PB) {
+        float2* pb = buf + PL::pad(base);
+        static_for<0, R>([&](auto rc) {
+          constexpr int r = decltype(rc)::value;
+          constexpr int off = (S % PB == 0) ? r * S + ((r * S) >> PL::PADSH) : r * S;
+          pb[off] = v[b * R + r];
+        });
+      } else {
+        static_for<0, R>([&](auto rc) {
+          constexpr int r = decltype(rc)::value;
+          buf[PL::pad(base + r * S)] = v[b * R + r];
+        });
+      }
     });
     team_sync<P>(mask);
     // load pass-(p+1) inputs, apply twiddles, bit-reverse into the register DFT order
@@ -272,9 +284,18 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
       constexpr int b = decltype(bc)::value;
       const int j = t + P * b;
       const int jm = j % Sn;
+      // j < L / Rn: with L / Rn a multiple of 2^PADSH the q-th input sits at a compile-time
+      // offset from pad(j)
+      constexpr int QS = L / Rn;
+      const float2* pj = buf + PL::pad(j);
       static_for<0, Rn>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
-        float2 val = buf[PL::pad(j + q * (L / Rn))];
+        float2 val;
+        if constexpr (QS % PB == 0) {
+          val = pj[q * QS + ((q * QS) >> PL::PADSH)];
+        } else {
+          val = buf[PL::pad(j + q * QS)];
+        }
         if constexpr (q > 0) val = cmul(val, twp[q * Sn + jm]);
         v[b * Rn + bitrev(q, ilog2(Rn))] = val;
       });
