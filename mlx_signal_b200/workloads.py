@@ -33,6 +33,13 @@ def _welch(msig, k):
     return [lambda: msig.welch(x, fs=48000.0, nperseg=1024)] * k
 
 
+def _welch_n(nperseg):
+    def build(msig, k):
+        x = _big()
+        return [lambda: msig.welch(x, fs=48000.0, nperseg=nperseg)] * k
+    return build
+
+
 def _stft(msig, k):
     x = _big()
     return [lambda: msig.stft(x, nperseg=1024)] * k
@@ -92,6 +99,8 @@ def _blue_stft(msig, k):
 #: name -> builder(msig, repeat) returning the calls to run
 WORKLOADS = {
     "welch_64x2p20_n1024": _welch,
+    "welch_64x2p20_n256": _welch_n(256),
+    "welch_64x2p20_n4096": _welch_n(4096),
     "stft_64x2p20": _stft,
     "spectrogram_64x2p20": _spectrogram,
     "coherence_64x2p20": _coherence,
