@@ -495,11 +495,9 @@ def general_shapes(x, dist, clocks, peak):
     import scipy.signal as sps
 
     import mlx_signal_b200 as msig
-    from mlx_signal_b200 import _kernels
 
     res = {}
     nps = 1000
-    nseg = (NSAMP - nps) // (nps // 2) + 1
     b = C * NSAMP * 4 + C * (nps // 2 + 1) * 4
     ms = timed(lambda: msig.welch(x, fs=FS, nperseg=nps), 10, 3, dist, clocks)
     # the same call on the composed path (what non-power-of-two shapes cost without the kernels)
@@ -526,7 +524,6 @@ def general_shapes(x, dist, clocks, peak):
         p = p.cpu().numpy()
         m = p_ref > 1e-6 * p_ref.max(axis=-1, keepdims=True)
         res["welch_64x2p20_n1000"]["max_rel_err"] = float(np.max(np.abs(p - p_ref)[m] / p_ref[m]))
-    _ = nseg, _kernels
     return res
 
 

@@ -6,8 +6,6 @@ is a fixed static device array. This file is collected last so that a run stoppi
 first failure has already run every other test; it also passes alone in a fresh process.
 """
 
-import ctypes
-
 import numpy as np
 import pytest
 import torch
