@@ -1,0 +1,119 @@
+"""GPU parity over seeded random argument combinations against float64 scipy.signal: welch,
+csd, coherence, spectrogram and stft with random rows, lengths, nperseg (powers of two and
+not), noverlap, nfft, detrend, window, scaling, real / complex input, mean / median averaging
+and boundary / padding. Each case uses the reference's tolerance rule (rtol 1e-4, atol 1e-5 of
+the peak; csd 2e-4, coherence 1e-3)."""
+
+import warnings
+
+import numpy as np
+import pytest
+import scipy.signal as sps
+
+import mlx_signal_b200 as msig
+from _utils import assert_close
+
+pytestmark = pytest.mark.gpu
+
+WINDOWS = ["hann", "hamming", "blackman", ("tukey", 0.3), "boxcar", ("kaiser", 6.0)]
+NPERSEGS = [1, 2, 7, 16, 33, 64, 100, 128, 250, 256, 300, 512, 777, 1000, 1024, 2048]
+
+
+def _case(rng):
+    nperseg = int(rng.choice(NPERSEGS))
+    n = int(rng.integers(nperseg, 6 * nperseg + 50))
+    rows = int(rng.integers(1, 4))
+    kw = {"nperseg": nperseg, "window": WINDOWS[int(rng.integers(len(WINDOWS)))]}
+    if nperseg > 1 and rng.random() < 0.6:
+        kw["noverlap"] = int(rng.integers(0, nperseg))
+    if rng.random() < 0.3:
+        kw["nfft"] = nperseg + int(rng.integers(0, nperseg + 1))
+    kw["detrend"] = [False, "constant", "linear"][int(rng.integers(3))]
+    cplx = rng.random() < 0.25
+    return rows, n, kw, cplx
+
+
+def _degenerate(kw) -> bool:
+    """Linear detrend of one- or two-sample segments leaves exact zeros: every output is
+    rounding residue (float64 in scipy, float32 here), checked against the input's scale."""
+    return kw["detrend"] == "linear" and kw["nperseg"] <= 2
+
+
+def _assert_residue(got, x, power: bool):
+    a = np.abs(got.cpu().numpy())
+    scale = float(np.max(np.abs(x))) ** (2 if power else 1)
+    assert a.max() <= 1e-5 * scale, f"degenerate case: output {a.max():.3e} vs scale {scale:.3e}"
+
+
+def _signal(rng, rows, n, cplx):
+    x = rng.standard_normal((rows, n)).astype(np.float32)
+    x += (rng.standard_normal((rows, 1)) * 2).astype(np.float32)  # DC offsets
+    if cplx:
+        x = (x + 1j * rng.standard_normal((rows, n))).astype(np.complex64)
+    return x
+
+
+@pytest.mark.parametrize("seed", range(60))
+def test_random_welch_csd_coherence(seed):
+    rng = np.random.default_rng(1000 + seed)
+    rows, n, kw, cplx = _case(rng)
+    x = _signal(rng, rows, n, cplx)
+    y = (0.6 * np.roll(x, 3, axis=-1) + 0.4 * _signal(rng, rows, n, cplx)).astype(x.dtype)
+    x64 = x.astype(np.complex128 if cplx else np.float64)
+    y64 = y.astype(np.complex128 if cplx else np.float64)
+    average = "median" if rng.random() < 0.3 else "mean"
+    scaling = "spectrum" if rng.random() < 0.3 else "density"
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _, p_ref = sps.welch(x64, fs=100.0, average=average, scaling=scaling, **kw)
+        _, p = msig.welch(x, fs=100.0, average=average, scaling=scaling, **kw)
+        assert tuple(p.shape) == p_ref.shape
+        _, c_ref = sps.csd(x64, y64, fs=100.0, average=average, scaling=scaling, **kw)
+        _, c = msig.csd(x, y, fs=100.0, average=average, scaling=scaling, **kw)
+        assert tuple(c.shape) == c_ref.shape
+        if _degenerate(kw):
+            _assert_residue(p, x, True)
+            _assert_residue(c, x, True)
+            return
+        assert_close(p, p_ref)
+        assert_close(c, c_ref, rtol=2e-4)
+        if kw["nperseg"] > 1:
+            _, h_ref = sps.coherence(x64, y64, fs=100.0, **kw)
+            _, h = msig.coherence(x, y, fs=100.0, **kw)
+            # bins whose auto-spectra are rounding residue (the DC bin of a boxcar window after
+            # detrending is exactly zero) have an undefined ratio: compare the others
+            _, pxx = sps.welch(x64, fs=100.0, **kw)
+            _, pyy = sps.welch(y64, fs=100.0, **kw)
+            keep = ((pxx > 1e-9 * pxx.max(axis=-1, keepdims=True))
+                    & (pyy > 1e-9 * pyy.max(axis=-1, keepdims=True)))
+            assert tuple(h.shape) == h_ref.shape
+            hh = h.cpu().numpy()
+            np.testing.assert_allclose(hh[keep], h_ref[keep], rtol=1e-3, atol=1e-5)
+
+
+@pytest.mark.parametrize("seed", range(60))
+def test_random_stft_spectrogram(seed):
+    rng = np.random.default_rng(2000 + seed)
+    rows, n, kw, cplx = _case(rng)
+    x = _signal(rng, rows, n, cplx)
+    x64 = x.astype(np.complex128 if cplx else np.float64)
+    boundary = [None, "zeros", "even", "odd", "constant"][int(rng.integers(5))]
+    if boundary in ("even", "odd") and kw["nperseg"] // 2 > n - 1:
+        boundary = "zeros"
+    padded = bool(rng.random() < 0.5)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _, t_ref, z_ref = sps.stft(x64, fs=50.0, boundary=boundary, padded=padded, **kw)
+        _, t, z = msig.stft(x, fs=50.0, boundary=boundary, padded=padded, **kw)
+        assert tuple(z.shape) == z_ref.shape
+        assert_close(t, t_ref)
+        mode = ["psd", "complex", "magnitude"][int(rng.integers(3))]
+        _, _, s_ref = sps.spectrogram(x64, fs=50.0, mode=mode, **kw)
+        _, _, s = msig.spectrogram(x, fs=50.0, mode=mode, **kw)
+        assert tuple(s.shape) == s_ref.shape
+        if _degenerate(kw):
+            _assert_residue(z, x, False)
+            _assert_residue(s, x, mode == "psd")
+            return
+        assert_close(z, z_ref)
+        assert_close(s, s_ref)
