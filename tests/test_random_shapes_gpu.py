@@ -117,3 +117,70 @@ def test_random_stft_spectrogram(seed):
             return
         assert_close(z, z_ref)
         assert_close(s, s_ref)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_istft(seed):
+    rng = np.random.default_rng(3000 + seed)
+    nperseg = int(rng.choice([8, 16, 64, 100, 128, 256, 512, 1024]))
+    noverlap = int(rng.integers(nperseg // 2, nperseg)) if rng.random() < 0.7 else nperseg // 2
+    window = WINDOWS[int(rng.integers(len(WINDOWS)))]
+    if window == "boxcar" and noverlap == 0:
+        noverlap = nperseg // 2
+    rows = int(rng.integers(1, 4))
+    n = int(rng.integers(nperseg, 6 * nperseg))
+    onesided = bool(rng.random() < 0.8)
+    x = rng.standard_normal((rows, n))
+    if not onesided:
+        x = x + 1j * rng.standard_normal((rows, n))
+    boundary = bool(rng.random() < 0.7)
+    kw = dict(window=window, nperseg=nperseg, noverlap=noverlap)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        _, _, z = sps.stft(x, return_onesided=onesided, boundary="zeros" if boundary else None,
+                           **kw)
+        t_ref, x_ref = sps.istft(z, input_onesided=onesided, boundary=boundary, **kw)
+        zc = z.astype(np.complex64)
+        t, xr = msig.istft(zc, input_onesided=onesided, boundary=boundary, **kw)
+    assert tuple(xr.shape) == x_ref.shape
+    # the overlap-added window energy the reconstruction divides by (scipy's NOLA norm): where
+    # it is small, float32 rounding of the frames is amplified by 1/norm, so those samples get a
+    # proportionally wider bound
+    w2 = sps.get_window(window, nperseg) ** 2
+    hop = nperseg - noverlap
+    nseg = z.shape[-1]
+    norm = np.zeros(nperseg + (nseg - 1) * hop)
+    for k in range(nseg):
+        norm[k * hop : k * hop + nperseg] += w2
+    if boundary:
+        norm = norm[nperseg // 2 : -(nperseg // 2)]
+    norm = norm[: x_ref.shape[-1]]
+    got = xr.cpu().numpy()
+    peak = float(np.max(np.abs(x_ref)))
+    well = norm >= 1e-2 * norm.max()
+    np.testing.assert_allclose(got[..., well], x_ref[..., well], rtol=1e-4, atol=1e-5 * peak)
+    bound = 1e-5 * peak * norm.max() / np.maximum(norm, 1e-10)
+    assert np.all(np.abs(got - x_ref) <= bound + 1e-4 * np.abs(x_ref))
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_convolutions(seed):
+    rng = np.random.default_rng(4000 + seed)
+    n1 = int(rng.integers(1, 30000))
+    n2 = int(rng.choice([1, 2, 5, 64, 129, 500, 1025, 2049, 3000, int(rng.integers(1, 5000))]))
+    rows = int(rng.integers(1, 3))
+    a = rng.standard_normal((rows, n1)).astype(np.float32)
+    b = rng.standard_normal((1, n2)).astype(np.float32)
+    if rng.random() < 0.3:
+        a, b = b, a  # filter first
+    mode = ["full", "same", "valid"][int(rng.integers(3))]
+    if mode == "valid" and not (all(p >= q for p, q in zip(a.shape, b.shape))
+                                or all(p <= q for p, q in zip(a.shape, b.shape))):
+        mode = "full"
+    fn = "oaconvolve" if rng.random() < 0.5 else "fftconvolve"
+    ref = getattr(sps, fn)(a.astype(np.float64), b.astype(np.float64), mode=mode, axes=-1)
+    got = getattr(msig, fn)(a, b, mode=mode, axes=-1)
+    assert tuple(got.shape) == ref.shape
+    if ref.size:
+        err = float(np.max(np.abs(got.cpu().numpy() - ref)) / max(np.max(np.abs(ref)), 1e-30))
+        assert err < 5e-6, f"{fn} {a.shape} {b.shape} {mode}: {err:.3e}"
