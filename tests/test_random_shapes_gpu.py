@@ -184,3 +184,56 @@ def test_random_convolutions(seed):
     if ref.size:
         err = float(np.max(np.abs(got.cpu().numpy() - ref)) / max(np.max(np.abs(ref)), 1e-30))
         assert err < 5e-6, f"{fn} {a.shape} {b.shape} {mode}: {err:.3e}"
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_batches(seed):
+    """welch_batch over a random mix (batched classes, other nperseg, short rows, windows,
+    detrend) against scipy per request."""
+    from mlx_signal_b200 import batch
+
+    rng = np.random.default_rng(5000 + seed)
+    items = []
+    for _ in range(int(rng.integers(1, 24))):
+        nps = int(rng.choice([256, 512, 1024, 4096, 300, 128]))
+        n = int(rng.integers(max(1, nps // 2), 5 * nps + 100))
+        x = rng.standard_normal((int(rng.integers(1, 5)), n)).astype(np.float32)
+        kw = {"nperseg": nps, "detrend": [False, "constant"][int(rng.integers(2))],
+              "window": ["hann", "hamming", ("tukey", 0.25)][int(rng.integers(3))]}
+        if rng.random() < 0.3:
+            kw["noverlap"] = int(rng.integers(0, min(nps, n)))
+        items.append((x, kw))
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        res = batch.welch_batch(items)
+        for (x, kw), (f, p) in zip(items, res):
+            f_ref, p_ref = sps.welch(x.astype(np.float64), **kw)
+            assert tuple(p.shape) == p_ref.shape
+            assert_close(f, f_ref)
+            assert_close(p, p_ref)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_streams(seed):
+    rng = np.random.default_rng(6000 + seed)
+    nps = int(rng.choice([256, 512, 1024, 4096, 200, 333]))
+    nov = int(rng.integers(0, nps))
+    rows = int(rng.integers(1, 4))
+    total = int(rng.integers(nps, 12 * nps))
+    x = rng.standard_normal((rows, total)).astype(np.float32)
+    st = msig.StreamingSTFT(rows=rows, fs=10.0, nperseg=nps, noverlap=nov)
+    sw = msig.StreamingWelch(rows=rows, fs=10.0, nperseg=nps, noverlap=nov)
+    pos, zs = 0, []
+    while pos < total:
+        m = int(rng.integers(0, 3 * nps))
+        chunk = x[:, pos : pos + m]
+        zs.append(st.push(chunk)[1].cpu().numpy())
+        sw.push(chunk)
+        pos += m
+    _, _, z_ref = sps.stft(x.astype(np.float64), fs=10.0, nperseg=nps, noverlap=nov,
+                           boundary=None, padded=False)
+    z = np.concatenate(zs, axis=-1)
+    assert z.shape == z_ref.shape
+    assert_close(z, z_ref)
+    _, p_ref = sps.welch(x.astype(np.float64), fs=10.0, nperseg=nps, noverlap=nov)
+    assert_close(sw.psd()[1], p_ref)
