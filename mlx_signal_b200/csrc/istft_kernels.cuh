@@ -198,9 +198,28 @@ struct IstftHalfCfg {
   static constexpr int TEAMS = PL::P >= 64 ? 1 : 128 / PL::P;
   static constexpr int THREADS = TEAMS * PL::P;
   static constexpr int H = PL::L / 2 > 0 ? PL::L / 2 : 1;
-  static constexpr size_t SMEM = size_t(PL::L) * 4 + size_t(H) * 4 * 3 + size_t(PL::TW) * 8 +
-                                 size_t(TEAMS) * PL::BUF * 8;
+  // per-team staging of one frame pair's one-sided spectra (bins 0..L/2), filled by cp.async
+  static constexpr int NBP = PL::L / 2 + 2;
+  static constexpr int STAGE = 2 * NBP;
+  // float tables (window, three norm tables) rounded to 16 bytes so the complex arrays after
+  // them stay 8-byte aligned (at L = 2 the tables are 5 floats)
+  static constexpr int FLT = (PL::L + 3 * H + 3) & ~3;
+  static constexpr size_t SMEM = size_t(FLT) * 4 + size_t(PL::TW) * 8 +
+                                 size_t(TEAMS) * PL::BUF * 8 + size_t(TEAMS) * STAGE * 8;
 };
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
 
 template <class PL>
 __device__ __forceinline__ void istft_load_pair(float2 (&v)[PL::E], const float2* za,
@@ -229,6 +248,33 @@ __device__ __forceinline__ void istft_load_pair(float2 (&v)[PL::E], const float2
   });
 }
 
+// istft_load_pair from a staged pair (sa, sb: one-sided bins of frames s, s+1 in shared memory)
+template <class PL>
+__device__ __forceinline__ void istft_stage_pair(float2 (&v)[PL::E], const float2* sa,
+                                                 const float2* sb, bool two, int nbins_in, int t) {
+  constexpr int L = PL::L;
+  static_for<0, PL::E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    const int k = slot_elem<PL, e>(t);
+    const bool upper = k > L / 2;
+    const int kk = upper ? L - k : k;
+    float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+    if (kk < nbins_in) {
+      a = sa[kk];
+      if (two) b = sb[kk];
+    }
+    if (kk == 0 || 2 * kk == L) {
+      a.y = 0.f;
+      b.y = 0.f;
+    }
+    if (upper) {
+      a.y = -a.y;
+      b.y = -b.y;
+    }
+    v[e] = make_float2(a.x - b.y, -(a.y + b.x));
+  });
+}
+
 template <int LOG_L, int LOG_E>
 __global__ void __launch_bounds__(IstftHalfCfg<LOG_L, LOG_E>::THREADS)
     k_istft_half(IstftParams pr) {
@@ -241,8 +287,9 @@ __global__ void __launch_bounds__(IstftHalfCfg<LOG_L, LOG_E>::THREADS)
   float* inv_mid = weff + L;                     // 1 / (w^2[n] + w^2[n+H]) or 1
   float* inv_first = inv_mid + H;                // 1 / w^2[n]      (block 0)
   float* inv_last = inv_first + H;               // 1 / w^2[n + H]  (block nseg)
-  float2* tw = reinterpret_cast<float2*>(inv_last + H);
+  float2* tw = reinterpret_cast<float2*>(weff + CFG::FLT);
   float2* sbuf = tw + PL::TW;
+  float2* stage_all = sbuf + CFG::TEAMS * PL::BUF;
   const float fs = pr.scale / float(L);
   for (int i = threadIdx.x; i < L; i += blockDim.x) weff[i] = pr.win[i] * fs;
   for (int i = threadIdx.x; i < H; i += blockDim.x) {
@@ -257,6 +304,8 @@ __global__ void __launch_bounds__(IstftHalfCfg<LOG_L, LOG_E>::THREADS)
   const int team = threadIdx.x / P, t = threadIdx.x - team * P;
   const unsigned mask = team_mask<P>();
   float2* buf = sbuf + team * PL::BUF;
+  float2* stage = stage_all + team * CFG::STAGE;  // [frame s | frame s+1][NBP]
+  const int nb_stage = pr.nbins_in < CFG::NBP ? pr.nbins_in : CFG::NBP;
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
@@ -279,17 +328,33 @@ __global__ void __launch_bounds__(IstftHalfCfg<LOG_L, LOG_E>::THREADS)
       for (int e = 0; e < EH; ++e) carry[e] = v[e + EH].x * weff[t + e * P + H];
       team_sync<P>(mask);
     }
+    // the pair's one-sided spectra are copied into the team's stage asynchronously (each bin
+    // once, coalesced), one pair ahead of the transform that reads them
+    auto issue = [&](int s) {
+      const float2* za = zr + int64_t(s) * pr.ldf;
+      const bool two = s + 1 < f1;
+      for (int i = t; i < nb_stage; i += P) {
+        cp_async8(stage + i, za + i);
+        if (two) cp_async8(stage + CFG::NBP + i, za + pr.ldf + i);
+      }
+      cp_async_commit();
+    };
+    if (f0 < f1) issue(f0);
     for (int s = f0; s < f1; s += 2) {
       const bool two = s + 1 < f1;
       const float2* za = zr + int64_t(s) * pr.ldf;
-      if (s + 3 < f1) {  // warm L2 with the next pair's two frames
-        const char* nx = reinterpret_cast<const char*>(za + 2 * int64_t(pr.ldf));
+      if (s + 5 < f1) {  // warm L2 with the pair after the one being staged next
+        const char* nx = reinterpret_cast<const char*>(za + 4 * int64_t(pr.ldf));
         const int bytes = 2 * pr.ldf * 8;
         for (int o = t * 128; o < bytes; o += P * 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(nx + o));
       }
+      cp_async_wait_all();
+      team_sync<P>(mask);
       float2 v[E];
-      istft_load_pair<PL>(v, za, za + pr.ldf, two, pr.nbins_in, t);
+      istft_stage_pair<PL>(v, stage, stage + CFG::NBP, two, nb_stage, t);
+      team_sync<P>(mask);  // every lane has read the stage: the next pair may overwrite it
+      if (s + 2 < f1) issue(s + 2);
       team_pass0<PL>(v);
       team_passes<PL>(v, buf, tw, t, mask);
       float* ob = orow + int64_t(s) * H;
