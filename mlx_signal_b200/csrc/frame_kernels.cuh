@@ -148,33 +148,51 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
         v[0] = csub(v[0], cmul(m, wlo[t]));
         v[E - 1] = csub(v[E - 1], cmul(m, whi[t]));
       }
-#pragma unroll
-      for (int e = 0; e < E; ++e) buf[PL::pad(t + e * P)] = v[e];
-      team_sync<P>(mask);
       const int64_t fa = r * pr.nseg + s;  // output frame index of segment a
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
+      auto emit = [&](int e) {
         const int k = t + e * P;
-        if (k < pr.nbins) {
-          const float2 z = v[e];
-          const float2 m = buf[PL::pad((L - k) & (L - 1))];
-          // a = (z + conj m)/2 ; b = (z - conj m)/(2i) = ((z.y + m.y), -(z.x - m.x)) / 2
-          const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
-          const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
-          if constexpr (KIND == kFrameStft) {
-            float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
-            oa[k] = xa;
-            if (two) oa[pr.nbins + k] = xb;
-          } else if constexpr (KIND == kFramePower) {
-            const float f = (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f;
-            float* oa = pr.out + fa * pr.nbins;
-            oa[k] = f * fmaf(xa.x, xa.x, xa.y * xa.y);
-            if (two) oa[pr.nbins + k] = f * fmaf(xb.x, xb.x, xb.y * xb.y);
-          } else {
-            // conj(X) Y per frame (no one-sided factor: applied after averaging)
-            float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
-            oa[k] = make_float2(fmaf(xa.x, xb.x, xa.y * xb.y), fmaf(xa.x, xb.y, -xa.y * xb.x));
-          }
+        const float2 z = v[e];
+        const float2 m = buf[PL::pad((L - k) & (L - 1))];
+        // a = (z + conj m)/2 ; b = (z - conj m)/(2i) = ((z.y + m.y), -(z.x - m.x)) / 2
+        const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
+        const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+        if constexpr (KIND == kFrameStft) {
+          float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
+          oa[k] = xa;
+          if (two) oa[pr.nbins + k] = xb;
+        } else if constexpr (KIND == kFramePower) {
+          const float f = (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f;
+          float* oa = pr.out + fa * pr.nbins;
+          oa[k] = f * fmaf(xa.x, xa.x, xa.y * xa.y);
+          if (two) oa[pr.nbins + k] = f * fmaf(xb.x, xb.x, xb.y * xb.y);
+        } else {
+          // conj(X) Y per frame (no one-sided factor: applied after averaging)
+          float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
+          oa[k] = make_float2(fmaf(xa.x, xb.x, xa.y * xb.y), fmaf(xa.x, xb.y, -xa.y * xb.x));
+        }
+      };
+      bool done = false;
+      if constexpr (E >= 2) {
+        if (pr.nbins == L / 2 + 1) {
+          // one-sided: bins k <= L/2 sit in registers e <= E/2 (k = L/2 only at t = 0), their
+          // mirrors in registers e >= E/2; bin 0 is its own mirror
+#pragma unroll
+          for (int e = E / 2; e < E; ++e) buf[PL::pad(t + e * P)] = v[e];
+          if (t == 0) buf[0] = v[0];
+          team_sync<P>(mask);
+#pragma unroll
+          for (int e = 0; e < E / 2; ++e) emit(e);
+          if (t == 0) emit(E / 2);
+          done = true;
+        }
+      }
+      if (!done) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) buf[PL::pad(t + e * P)] = v[e];
+        team_sync<P>(mask);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          if (t + e * P < pr.nbins) emit(e);
         }
       }
       team_sync<P>(mask);
@@ -290,28 +308,42 @@ __device__ __forceinline__ void frames_half_range(const HalfCtx<PL>& c, const Fr
       v[0] = csub(v[0], cmul(m, c.wlo[t]));
       v[E - 1] = csub(v[E - 1], cmul(m, c.whi[t]));
     }
-#pragma unroll
-    for (int e = 0; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
-    team_sync<P>(c.mask);
     const int64_t fa = r * pr.nseg + s;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
+    // bin k of frames s (a) and s+1 (b) from the packed Z_k and its mirror Z_{L-k}
+    auto emit = [&](int e) {
       const int k = t + e * P;
-      if (k < pr.nbins) {
-        const float2 z = v[e];
-        const float2 m = c.buf[PL::pad((L - k) & (L - 1))];
-        const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
-        const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
-        if constexpr (KIND == kFrameStft) {
-          float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
-          oa[k] = xa;
-          if (TWO) oa[pr.nbins + k] = xb;
-        } else {
-          const float f = (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f;
-          float* oa = pr.out + fa * pr.nbins;
-          oa[k] = f * fmaf(xa.x, xa.x, xa.y * xa.y);
-          if (TWO) oa[pr.nbins + k] = f * fmaf(xb.x, xb.x, xb.y * xb.y);
-        }
+      const float2 z = v[e];
+      const float2 m = c.buf[PL::pad((L - k) & (L - 1))];
+      const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
+      const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
+      if constexpr (KIND == kFrameStft) {
+        float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
+        oa[k] = xa;
+        if (TWO) oa[pr.nbins + k] = xb;
+      } else {
+        const float f = (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f;
+        float* oa = pr.out + fa * pr.nbins;
+        oa[k] = f * fmaf(xa.x, xa.x, xa.y * xa.y);
+        if (TWO) oa[pr.nbins + k] = f * fmaf(xb.x, xb.x, xb.y * xb.y);
+      }
+    };
+    if (pr.nbins == L / 2 + 1 && E >= 2) {
+      // one-sided: bins k <= L/2 sit in registers e <= E/2 (k = L/2 only at t = 0); their
+      // mirrors L - k in registers e >= E/2, and bin 0 is its own mirror
+#pragma unroll
+      for (int e = E / 2; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
+      if (t == 0) c.buf[0] = v[0];
+      team_sync<P>(c.mask);
+#pragma unroll
+      for (int e = 0; e < E / 2; ++e) emit(e);
+      if (t == 0) emit(E / 2);
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
+      team_sync<P>(c.mask);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        if (t + e * P < pr.nbins) emit(e);
       }
     }
     team_sync<P>(c.mask);
