@@ -276,8 +276,10 @@ __device__ __forceinline__ void batch_item(const BatchReqDev* __restrict__ rq, i
       });
       team_pass0<PL>(v);
       team_passes<PL>(v, c.buf, c.tw, t, c.mask);
+      // mirrors of the one-sided bins k <= L/2: registers e >= E/2, and bin 0 itself
 #pragma unroll
-      for (int e = 0; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
+      for (int e = E / 2; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
+      if (t == 0) c.buf[0] = v[0];
       team_sync<P>(c.mask);
       float2* oa = orow + int64_t(s) * NB;
 #pragma unroll
