@@ -180,9 +180,9 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_welch(MeanPara
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
-  float acc[E];
+  float acc[E / 2];  // bins k = t + e P < N <= M/2
 #pragma unroll
-  for (int e = 0; e < E; ++e) acc[e] = 0.f;
+  for (int e = 0; e < E / 2; ++e) acc[e] = 0.f;
   while (g < gend) {
     const int64_t r = g / pr.nseg;
     const int s0 = int(g - r * pr.nseg);
@@ -202,8 +202,9 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_welch(MeanPara
       });
       blue_premultiply<PL, DET>(v, sm.cin, pr.nperseg, t, scratch, mask);
       blue_core<PL>(v, bh, buf, sm.tw, t, mask);
+      // bins k < N <= M/2 live in registers e < E/2 (k = t + e P)
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
+      for (int e = 0; e < E / 2; ++e) {
         acc[e] = fmaf(v[e].x, v[e].x, acc[e]);
         acc[e] = fmaf(v[e].y, v[e].y, acc[e]);
       }
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_welch(MeanPara
     float* sq = reinterpret_cast<float*>(buf);
     team_sync<P>(mask);
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
+    for (int e = 0; e < E / 2; ++e) {
       sq[t + e * P] = acc[e];
       acc[e] = 0.f;
     }
@@ -277,9 +278,9 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_frames(FramePa
       }
       blue_premultiply<PL, DET>(v, sm.cin, pr.nperseg, t, scratch, mask);
       blue_core<PL>(v, bh, buf, sm.tw, t, mask);
-      // Z_k = d_k conj(V_k), k < N, staged for the mirror read Z_{N-k}
+      // Z_k = d_k conj(V_k), k < N (registers e < E/2), staged for the mirror read Z_{N-k}
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
+      for (int e = 0; e < E / 2; ++e) {
         const int k = t + e * P;
         if (k < N) {
           const float2 d = sm.cout[k];
@@ -290,7 +291,7 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_frames(FramePa
       team_sync<P>(mask);
       const int64_t fa = r * pr.nseg + s;
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
+      for (int e = 0; e < E / 2; ++e) {
         const int k = t + e * P;
         if (k < pr.nbins) {
           const float2 z = v[e];
@@ -334,10 +335,10 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_cross(MeanPara
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
-  float q[E];
-  float2 c[E];
+  float q[E / 2];  // bins k = t + e P < N <= M/2
+  float2 c[E / 2];
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
+  for (int e = 0; e < E / 2; ++e) {
     q[e] = 0.f;
     c[e] = make_float2(0.f, 0.f);
   }
@@ -362,7 +363,7 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_cross(MeanPara
       blue_premultiply<PL, DET>(v, sm.cin, pr.nperseg, t, scratch, mask);
       blue_core<PL>(v, bh, buf, sm.tw, t, mask);
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
+      for (int e = 0; e < E / 2; ++e) {
         const int k = t + e * P;
         if (k < N) {
           q[e] = fmaf(v[e].x, v[e].x, fmaf(v[e].y, v[e].y, q[e]));
@@ -372,7 +373,7 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_cross(MeanPara
       }
       team_sync<P>(mask);
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
+      for (int e = 0; e < E / 2; ++e) {
         const int k = t + e * P;
         if (2 * k <= N) {
           const float2 m = buf[PL::pad(k == 0 ? 0 : N - k)];
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(BlueCfg<LOG_M>::THREADS) k_blue_cross(MeanPara
     float* dst = pr.partial + (r * pr.cmax + slot) * int64_t(cross_slot_floats(N));
     float2* dstc = reinterpret_cast<float2*>(dst + cross_q_floats(N));
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
+    for (int e = 0; e < E / 2; ++e) {
       const int k = t + e * P;
       if (k < N) dst[k] = q[e];
       if (2 * k <= N) dstc[k] = c[e];
