@@ -433,13 +433,16 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
       detrend_window<PL, DET>(v, sm.win, t, pr.nperseg, scratch, mask);
       team_pass0<PL>(v);
       team_passes<PL>(v, buf, sm.tw, t, mask);
-      // mirror exchange through the (now free) buffer
+      // mirror exchange through the (now free) buffer: the mirrors L - k of the bins k <= L/2
+      // read below sit in registers e >= E/2 (bin 0 is its own mirror)
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         q[e] = fmaf(v[e].x, v[e].x, q[e]);
         q[e] = fmaf(v[e].y, v[e].y, q[e]);
-        buf[PL::pad(t + e * P)] = v[e];
       }
+#pragma unroll
+      for (int e = E / 2; e < E; ++e) buf[PL::pad(t + e * P)] = v[e];
+      if (t == 0) buf[0] = v[0];
       team_sync<P>(mask);
 #pragma unroll
       for (int e = 0; e < EH; ++e) {
@@ -608,8 +611,11 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
       for (int e = 0; e < E; ++e) {
         q[e] = fmaf(v[e].x, v[e].x, q[e]);
         q[e] = fmaf(v[e].y, v[e].y, q[e]);
-        buf[PL::pad(t + e * P)] = v[e];
       }
+      // mirrors L - k of the bins k <= L/2 read below: registers e >= E/2, and bin 0 itself
+#pragma unroll
+      for (int e = E / 2; e < E; ++e) buf[PL::pad(t + e * P)] = v[e];
+      if (t == 0) buf[0] = v[0];
       team_sync<P>(mask);
 #pragma unroll
       for (int e = 0; e < EH1; ++e) {
