@@ -313,7 +313,7 @@ SP_API int sp_conv_block_len(int n2);
  * must be zero-filled before its first run; every run leaves its queue and counters zero again,
  * and sp_batch_run's arguments do not depend on the batch, so one captured launch replays for
  * any batch encoded into the same descriptor buffer and workspace. Outputs must not alias
- * inputs or one another. Batched classes: nperseg == nfft in {256, 512, 1024, 4096}.
+ * inputs or one another. Batched classes: nperseg == nfft in {256, 512, 1024, 2048, 4096}.
  * ------------------------------------------------------------------------------------------ */
 enum { SP_BATCH_WELCH = 0, SP_BATCH_STFT_STREAM = 1 };
 

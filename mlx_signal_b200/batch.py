@@ -2,7 +2,7 @@
 kernel launch over a device work queue (C-ABI sp_batch_*, include/b200signal.h).
 
 * `prepare_welch(x, **welch_kwargs)` validates one welch call exactly as `welch` does and, when
-  it fits the batched kernel (real input, nperseg == nfft in {256, 512, 1024, 4096}, 50% overlap,
+  it fits the batched kernel (real input, nperseg == nfft in {256, 512, 1024, 2048, 4096}, 50% overlap,
   detrend False or 'constant', mean averaging), returns a `WelchJob` whose `result()` is what
   `welch` would return; otherwise None.
 * `StftStream` keeps a stream's overlap tail resident on the device (two ping-pong buffers per
@@ -47,7 +47,7 @@ __all__ = [
     "welch_batch",
 ]
 
-BATCH_NPERSEG = (256, 512, 1024, 4096)
+BATCH_NPERSEG = (256, 512, 1024, 2048, 4096)
 KIND_WELCH, KIND_STREAM = 0, 1
 
 

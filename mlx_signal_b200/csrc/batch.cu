@@ -15,9 +15,14 @@ namespace b2s {
 // once per device by k_batch_init (FP64 sincospi, rounded once, as the shared tables).
 using BatchPlan12 = Plan<12, batch_log_e<12>()>;
 __device__ float2 g_batch_tw12[BatchPlan12::TW];
+// the 2048 class's inter-pass twiddles exceed the shared-memory twiddle slot as well
+using BatchPlan11 = Plan<11, batch_log_e<11>()>;
+__device__ float2 g_batch_tw11[BatchPlan11::TW];
 
 __global__ void k_batch_init() {
   build_twiddles<BatchPlan12>(g_batch_tw12, int(blockIdx.x * blockDim.x + threadIdx.x),
+                              int(gridDim.x * blockDim.x));
+  build_twiddles<BatchPlan11>(g_batch_tw11, int(blockIdx.x * blockDim.x + threadIdx.x),
                               int(gridDim.x * blockDim.x));
 }
 
@@ -62,6 +67,7 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) k_batch(BatchP
       case 8: batch_item<8, batch_log_e<8>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
       case 9: batch_item<9, batch_log_e<9>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
       case 10: batch_item<10, batch_log_e<10>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
+      case 11: batch_item<11, batch_log_e<11>()>(rq, local, smem, cur, g_batch_tw11, s_rows, &s_nrows); break;
       case 12: batch_item<12, batch_log_e<12>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
       default: break;  // rejected by the encoder
     }
@@ -84,7 +90,7 @@ constexpr int64_t kQueueBytes = 256;
 
 bool batch_class(int nperseg, int* log_l) {
   const int l = ilog2_exact(nperseg);
-  if (l == 8 || l == 9 || l == 10 || l == 12) {
+  if (l == 8 || l == 9 || l == 10 || l == 11 || l == 12) {
     *log_l = l;
     return true;
   }
@@ -112,7 +118,7 @@ struct ReqPlan {
 
 int plan_request(const sp_batch_request& r, int idx, ReqPlan* p) {
   if (!batch_class(r.nperseg, &p->log_l)) {
-    set_error("request %d: nperseg=%d is not a batched class (256, 512, 1024, 4096)", idx,
+    set_error("request %d: nperseg=%d is not a batched class (256, 512, 1024, 2048, 4096)", idx,
               r.nperseg);
     return SP_ERR_UNSUPPORTED;
   }

@@ -37,7 +37,7 @@ def nseg_of(x, kw):
 def _mixed_requests(rng, k=24, max_log=17):
     reqs = []
     for _ in range(k):
-        N = int(rng.choice([256, 512, 1024, 4096]))
+        N = int(rng.choice([256, 512, 1024, 2048, 4096]))
         C = int(rng.integers(1, 7))
         n = int(2 ** rng.uniform(max(12, np.log2(N)), max_log))
         x = rng.standard_normal((C, n)).astype(np.float32)
@@ -73,7 +73,7 @@ def test_alone_and_in_mix_are_bit_identical(rng):
 
 def test_batch_agrees_with_single_request_path(rng):
     x = rng.standard_normal((5, 1 << 16)).astype(np.float32)
-    for N in (256, 512, 1024, 4096):
+    for N in (256, 512, 1024, 2048, 4096):
         (_, pb), = mb.welch_batch([x], nperseg=N)
         _, ps = msig.welch(x, nperseg=N)
         assert rel_err_bins(pb, ps.cpu().numpy().astype(np.float64)) <= 2e-6
@@ -89,7 +89,7 @@ def test_axis_and_outer_shape(rng):
 
 def test_ineligible_requests_use_the_regular_path(rng):
     x = rng.standard_normal(8192).astype(np.float32)
-    cases = [{"nperseg": 2048}, {"nperseg": 1024, "detrend": "linear"},
+    cases = [{"nperseg": 128}, {"nperseg": 1024, "detrend": "linear"},
              {"nperseg": 1024, "noverlap": 256}, {"nperseg": 300},
              {"nperseg": 1024, "average": "median"}]
     res = mb.welch_batch([(x, c) for c in cases])

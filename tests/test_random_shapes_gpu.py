@@ -195,7 +195,7 @@ def test_random_batches(seed):
     rng = np.random.default_rng(5000 + seed)
     items = []
     for _ in range(int(rng.integers(1, 24))):
-        nps = int(rng.choice([256, 512, 1024, 4096, 300, 128]))
+        nps = int(rng.choice([256, 512, 1024, 2048, 4096, 300, 128]))
         n = int(rng.integers(max(1, nps // 2), 5 * nps + 100))
         x = rng.standard_normal((int(rng.integers(1, 5)), n)).astype(np.float32)
         kw = {"nperseg": nps, "detrend": [False, "constant"][int(rng.integers(2))],
@@ -216,7 +216,7 @@ def test_random_batches(seed):
 @pytest.mark.parametrize("seed", range(12))
 def test_random_streams(seed):
     rng = np.random.default_rng(6000 + seed)
-    nps = int(rng.choice([256, 512, 1024, 4096, 200, 333]))
+    nps = int(rng.choice([256, 512, 1024, 2048, 4096, 200, 333]))
     nov = int(rng.integers(0, nps))
     rows = int(rng.integers(1, 4))
     total = int(rng.integers(nps, 12 * nps))
