@@ -149,10 +149,20 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
         v[E - 1] = csub(v[E - 1], cmul(m, whi[t]));
       }
       const int64_t fa = r * pr.nseg + s;  // output frame index of segment a
-      auto emit = [&](int e) {
+      // f: the one-sided factor of bin k (power kind only)
+      auto emit = [&](int e, float f) {
         const int k = t + e * P;
         const float2 z = v[e];
         const float2 m = buf[PL::pad((L - k) & (L - 1))];
+        if constexpr (KIND == kFramePower) {
+          // |X_a|^2 = |z + conj m|^2 / 4, |X_b|^2 = |z - conj m|^2 / 4
+          const float sc = 0.25f * f;
+          const float a1 = z.x + m.x, a2 = z.y - m.y, b1 = z.y + m.y, b2 = m.x - z.x;
+          float* oa = pr.out + fa * pr.nbins;
+          oa[k] = sc * fmaf(a1, a1, a2 * a2);
+          if (two) oa[pr.nbins + k] = sc * fmaf(b1, b1, b2 * b2);
+          return;
+        }
         // a = (z + conj m)/2 ; b = (z - conj m)/(2i) = ((z.y + m.y), -(z.x - m.x)) / 2
         const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
         const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
@@ -160,12 +170,7 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
           float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
           oa[k] = xa;
           if (two) oa[pr.nbins + k] = xb;
-        } else if constexpr (KIND == kFramePower) {
-          const float f = (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f;
-          float* oa = pr.out + fa * pr.nbins;
-          oa[k] = f * fmaf(xa.x, xa.x, xa.y * xa.y);
-          if (two) oa[pr.nbins + k] = f * fmaf(xb.x, xb.x, xb.y * xb.y);
-        } else {
+        } else if constexpr (KIND == kFrameCross) {
           // conj(X) Y per frame (no one-sided factor: applied after averaging)
           float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
           oa[k] = make_float2(fmaf(xa.x, xb.x, xa.y * xb.y), fmaf(xa.x, xb.y, -xa.y * xb.x));
@@ -180,9 +185,11 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
           for (int e = E / 2; e < E; ++e) buf[PL::pad(t + e * P)] = v[e];
           if (t == 0) buf[0] = v[0];
           team_sync<P>(mask);
+          // bins 0 < k < L/2 take the factor 2, DC (t = 0, e = 0) and Nyquist (e = E/2) 1
+          emit(0, t == 0 ? 1.f : 2.f);
 #pragma unroll
-          for (int e = 0; e < E / 2; ++e) emit(e);
-          if (t == 0) emit(E / 2);
+          for (int e = 1; e < E / 2; ++e) emit(e, 2.f);
+          if (t == 0) emit(E / 2, 1.f);
           done = true;
         }
       }
@@ -192,7 +199,8 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
         team_sync<P>(mask);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-          if (t + e * P < pr.nbins) emit(e);
+          const int k = t + e * P;
+          if (k < pr.nbins) emit(e, (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f);
         }
       }
       team_sync<P>(mask);
@@ -310,21 +318,24 @@ __device__ __forceinline__ void frames_half_range(const HalfCtx<PL>& c, const Fr
     }
     const int64_t fa = r * pr.nseg + s;
     // bin k of frames s (a) and s+1 (b) from the packed Z_k and its mirror Z_{L-k}
-    auto emit = [&](int e) {
+    // f: the one-sided factor of bin k (power kind only)
+    auto emit = [&](int e, float f) {
       const int k = t + e * P;
       const float2 z = v[e];
       const float2 m = c.buf[PL::pad((L - k) & (L - 1))];
-      const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
-      const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
       if constexpr (KIND == kFrameStft) {
+        const float2 xa = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
+        const float2 xb = make_float2(0.5f * (z.y + m.y), 0.5f * (m.x - z.x));
         float2* oa = reinterpret_cast<float2*>(pr.out) + fa * pr.nbins;
         oa[k] = xa;
         if (TWO) oa[pr.nbins + k] = xb;
       } else {
-        const float f = (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f;
+        // |X_a|^2 = |z + conj m|^2 / 4, |X_b|^2 = |z - conj m|^2 / 4
+        const float sc = 0.25f * f;
+        const float a1 = z.x + m.x, a2 = z.y - m.y, b1 = z.y + m.y, b2 = m.x - z.x;
         float* oa = pr.out + fa * pr.nbins;
-        oa[k] = f * fmaf(xa.x, xa.x, xa.y * xa.y);
-        if (TWO) oa[pr.nbins + k] = f * fmaf(xb.x, xb.x, xb.y * xb.y);
+        oa[k] = sc * fmaf(a1, a1, a2 * a2);
+        if (TWO) oa[pr.nbins + k] = sc * fmaf(b1, b1, b2 * b2);
       }
     };
     if (pr.nbins == L / 2 + 1 && E >= 2) {
@@ -334,16 +345,19 @@ __device__ __forceinline__ void frames_half_range(const HalfCtx<PL>& c, const Fr
       for (int e = E / 2; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
       if (t == 0) c.buf[0] = v[0];
       team_sync<P>(c.mask);
+      // bins 0 < k < L/2 take the factor 2, DC (t = 0, e = 0) and Nyquist (e = E/2) 1
+      emit(0, t == 0 ? 1.f : 2.f);
 #pragma unroll
-      for (int e = 0; e < E / 2; ++e) emit(e);
-      if (t == 0) emit(E / 2);
+      for (int e = 1; e < E / 2; ++e) emit(e, 2.f);
+      if (t == 0) emit(E / 2, 1.f);
     } else {
 #pragma unroll
       for (int e = 0; e < E; ++e) c.buf[PL::pad(t + e * P)] = v[e];
       team_sync<P>(c.mask);
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        if (t + e * P < pr.nbins) emit(e);
+        const int k = t + e * P;
+        if (k < pr.nbins) emit(e, (onesided && k != 0 && 2 * k != L) ? 2.f : 1.f);
       }
     }
     team_sync<P>(c.mask);
