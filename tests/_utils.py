@@ -22,8 +22,8 @@ def assert_close(actual, desired, rtol=1e-4, atol_frac=1e-5):
 
 
 def rel_err_bins(actual, desired, floor=1e-6):
-    """Max relative error over bins whose magnitude exceeds `floor` x the peak (the north-star
-    accuracy metric: <= 1e-5 on bins above 1e-6 of the peak)."""
+    """Max relative error over bins whose magnitude exceeds `floor` x the peak (the
+    accuracy bar of this project: <= 1e-5 on bins above 1e-6 of the peak)."""
     a = as_np(actual)
     a = a.astype(np.complex128 if np.iscomplexobj(a) else np.float64)
     d = np.asarray(desired)

@@ -1,8 +1,9 @@
 """Generate the golden fixtures: seeded float32 inputs and float64 scipy.signal outputs.
 
 The reference (mlx-signal) tests against float64 scipy computed in-test and ships no vectors;
-these fixtures freeze that oracle for the workloads of this project (BASELINE config 1 exactly,
-scaled-down configs 2 and 3, stft/istft/spectrogram cases). Run from the repo root:
+these fixtures freeze that oracle for the workloads of this project (the 1 x 2^16 welch case
+exactly, scaled-down versions of the 64 x 2^20 welch and cross-spectral workloads,
+stft/istft/spectrogram and packed rfft cases). Run from the repo root:
 
     python tests/golden/make_golden.py
 """
@@ -29,19 +30,19 @@ def multitone(rng, C, n, fs):
 def main():
     rng = np.random.default_rng(20261203)
     g = {}
-    # config 1: 1 x 2^16, N(0,1) + unit sinusoid at 0.1 fs; hann 256/128, constant, density
+    # small welch: 1 x 2^16, N(0,1) + unit sinusoid at 0.1 fs; hann 256/128, constant, density
     n1 = 1 << 16
     x1 = (rng.standard_normal(n1) + np.sin(2 * np.pi * 0.1 * np.arange(n1))).astype(np.float32)
     g["welch1_x"] = x1
     g["welch1_f"], g["welch1_p"] = sps.welch(x1.astype(np.float64), fs=1.0, window="hann",
                                              nperseg=256, noverlap=128, detrend="constant",
                                              scaling="density", average="mean")
-    # config 2 scaled down: 4 x 2^13 multi-tone, fs 48 kHz, hann 1024/512
+    # the 64 x 2^20 welch workload scaled down: 4 x 2^13 multi-tone, fs 48 kHz, hann 1024/512
     x2 = multitone(rng, 4, 1 << 13, 48000.0)
     g["welch2_x"] = x2
     g["welch2_f"], g["welch2_p"] = sps.welch(x2.astype(np.float64), fs=48000.0, nperseg=1024,
                                              noverlap=512)
-    # config 3 scaled down: y = 0.7 * circular shift(x) + 0.3 N(0,1)
+    # the cross-spectral (csd / coherence) workload scaled down: y = 0.7 * circular shift(x) + 0.3 N(0,1)
     x3 = rng.standard_normal((4, 1 << 14)).astype(np.float32)
     shifts = rng.integers(0, 65, size=4)
     y3 = np.stack([0.7 * np.roll(x3[c], int(shifts[c])) for c in range(4)])

@@ -1,5 +1,5 @@
 """GPU parity of the batched persistent launch: mixed welch requests against float64
-scipy.signal.welch (max relative error <= 1e-5 on bins above 1e-6 of the peak),
+scipy.signal.welch (accuracy bar: max relative error <= 1e-5 on bins above 1e-6 of the peak),
 bit-identical results alone and inside a mix, streaming-STFT chunks against scipy.signal.stft of
 the concatenated stream, graph replay of one captured launch for different batches, the queue
 returning to zero between launches, and the autotuner's cache entry."""

@@ -2,7 +2,7 @@
 
 Cases follow the reference's tests/test_spectral.py (WELCH_CASES, multidim axes, csd
 mean/median/broadcast/unequal, coherence, grouped-vs-scipy over nperseg 64..2048) and add the
-north-star accuracy bar (max relative error <= 1e-5 on bins above 1e-6 of the peak).
+float32 accuracy bar (max relative error <= 1e-5 on bins above 1e-6 of the peak).
 """
 
 import numpy as np
@@ -201,7 +201,7 @@ def test_fused_welch_every_size(rng, nfft, detrend):
                                atol=max(2e-5 * np.abs(c_ref).max(), floor))
 
 
-def test_welch_north_star_accuracy(rng):
+def test_welch_accuracy_bar(rng):
     """48 kHz multi-tone channels, hann, nperseg 1024 / 50%: <= 1e-5 relative on bins above
     1e-6 of the peak (scaled-down channel count of the 64 x 2^20 workload)."""
     fs = 48000.0
@@ -338,7 +338,7 @@ def test_bluestein_welch_matches_scipy(rng, kw):
     assert rel_err_bins(p, p_ref) <= 1e-5
 
 
-def test_bluestein_welch_north_star_shape(rng):
+def test_bluestein_welch_accuracy_bar(rng):
     """64 x 2^18 channels, nperseg 1000: the 1e-5 bar on bins above 1e-6 of the peak."""
     x = make_sig(rng, (64, 1 << 18))
     f_ref, p_ref = sps.welch(x.astype(np.float64), fs=48000, nperseg=1000)
