@@ -18,6 +18,7 @@ Results are float32 (complex64 if either input is complex) on the GPU.
 from __future__ import annotations
 
 import math
+import operator
 
 import numpy as np
 import torch
@@ -44,16 +45,20 @@ def _conv_len(n: int) -> int:
 
 
 def _init_axes(a1: torch.Tensor, a2: torch.Tensor, mode: str, axes):
-    """scipy's axis handling: default all axes, non-convolution axes must broadcast, 'valid'
-    needs one input at least as large as the other along every axis (swapped if needed), axes
-    where both sizes are 1 are dropped. Returns (a1, a2, axes)."""
+    """scipy's axis handling: default all axes, axes are integers (scalar or iterable), non-
+    convolution axes must broadcast, 'valid' needs one input at least as large as the other along
+    every axis (swapped if needed), axes where both sizes are 1 are dropped. Returns
+    (a1, a2, axes)."""
     if mode not in ("full", "same", "valid"):
         raise ValueError("acceptable mode flags are 'valid', 'same', or 'full'")
     nd = a1.dim()
     if axes is None:
         axes = list(range(nd))
     else:
-        axes = [int(a) for a in np.atleast_1d(axes)]
+        try:
+            axes = [operator.index(a) for a in np.atleast_1d(axes).tolist()]
+        except TypeError:
+            raise ValueError("axes must be a scalar or iterable of integers") from None
         axes = [a + nd if a < 0 else a for a in axes]
         if any(a < 0 or a >= nd for a in axes):
             raise ValueError("axes exceeds dimensionality of input")

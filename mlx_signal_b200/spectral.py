@@ -861,8 +861,7 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
         raise ValueError("noverlap must be less than nperseg.")
     nstep = nperseg - noverlap
     if isinstance(window, str | tuple):
-        key = tuple(window) if isinstance(window, tuple) else window
-        win_np = _window_np(key, nperseg)
+        win_np = _window_np(tuple(window) if isinstance(window, tuple) else window, nperseg)
     else:
         win_np = np.asarray(to_numpy(window), dtype=np.float64)
         if win_np.ndim != 1:

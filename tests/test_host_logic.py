@@ -116,6 +116,27 @@ def test_conv_ols_block_choice_and_argument_errors():
     assert lib.sp_conv_ols_f32(dummy, 0, 100, 100, dummy, 10, 0, 109, dummy, 109, None) == _lib.SP_OK
 
 
+def test_convolve_axes_validation():
+    """scipy's axis rules for fftconvolve / oaconvolve (the reference's
+    tests/test_edge_cases.py:246-256): integer axes only, in range, unique; singleton axes
+    dropped. Shapes only, so CPU tensors stand in for the device inputs."""
+    import torch
+
+    from mlx_signal_b200.convolution import _init_axes
+
+    a = torch.zeros((4, 5))
+    for bad, msg in ((2, "exceeds dimensionality"), ([-3], "exceeds dimensionality"),
+                     (1.5, "integers"), ([0.5, 1], "integers"), ([1, -1], "unique")):
+        with pytest.raises(ValueError, match=msg):
+            _init_axes(a, a, "full", bad)
+    assert _init_axes(a, a, "full", np.int64(1))[2] == [1]
+    assert _init_axes(a, a, "full", [np.int32(0), -1])[2] == [0, 1]
+    one = torch.zeros((1, 3))
+    assert _init_axes(one, one, "full", [0])[2] == []  # every conv axis is length 1: a product
+    with pytest.raises(ValueError, match="mode flags"):
+        _init_axes(a, a, "circular", None)
+
+
 def test_profiling_workloads_listed():
     from mlx_signal_b200 import workloads
 

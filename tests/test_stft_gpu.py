@@ -204,6 +204,63 @@ def test_istft_axis_and_dtype_validation(rng):
             msig.istft(z128, nperseg=128)
 
 
+def test_istft_memory_layouts_bit_identical(rng):
+    """Equivalent NumPy / torch layouts of one spectrogram give bit-identical istft outputs
+    (the reference's tests/test_spectral.py:395-423)."""
+    import warnings
+
+    x = make_sig(rng, (2, 3, 2048))
+    _, _, z_sp = sps.stft(x.astype(np.float64), nperseg=256)
+    z_sp = z_sp.astype(np.complex64)
+    _, x_ref = sps.istft(z_sp, nperseg=256)
+    t_base, y_base = msig.istft(z_sp, nperseg=256)
+    t_base, y_base = t_base.cpu().numpy(), y_base.cpu().numpy()
+    assert_close(y_base, x_ref)
+    z_ro = z_sp.copy()
+    z_ro.setflags(write=False)
+    variants = [
+        (np.ascontiguousarray(z_sp), {}),
+        (np.ascontiguousarray(np.swapaxes(z_sp, -2, -1)), {"time_axis": -2, "freq_axis": -1}),
+        (np.asfortranarray(z_sp), {}),
+        (np.transpose(z_sp, (2, 0, 1, 3)), {"freq_axis": 0, "time_axis": -1}),
+        (z_sp.astype(np.complex128), {}),
+        (z_ro, {}),
+        (torch.from_numpy(np.ascontiguousarray(z_sp)), {}),
+        (torch.from_numpy(np.ascontiguousarray(z_sp)).cuda(), {}),
+        (torch.from_numpy(np.ascontiguousarray(np.swapaxes(z_sp, -2, -1))).cuda().transpose(-2, -1),
+         {}),
+    ]
+    for arr, kw in variants:
+        for _ in range(2):  # the second CUDA call runs the cached plan
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore", msig.DowncastWarning)
+                t_got, y_got = msig.istft(arr, nperseg=256, **kw)
+            np.testing.assert_array_equal(t_got.cpu().numpy(), t_base)
+            np.testing.assert_array_equal(y_got.cpu().numpy(), y_base)
+
+
+def test_istft_strided_reversed_and_broadcast_views(rng):
+    """Sliced, reversed and broadcast views match scipy (the reference's
+    tests/test_spectral.py:426-441), as NumPy views and as torch CUDA views."""
+    x = make_sig(rng, (3, 2048))
+    _, _, z = sps.stft(x.astype(np.float64), nperseg=256)
+    z = z.astype(np.complex64)
+    zt = torch.from_numpy(np.ascontiguousarray(z)).cuda()
+    views = [
+        (z[:, :, ::2], zt[:, :, ::2]),
+        (z[:, :, ::-1], zt.flip(-1)),
+        (np.ascontiguousarray(z)[:, :, ::-1], None),
+        (np.broadcast_to(z[:1], (4,) + z.shape[1:]), zt[:1].expand((4,) + z.shape[1:])),
+        (z[::2, 3:, 1:-1], zt[::2, 3:, 1:-1]),
+    ]
+    for view, tview in views:
+        _, x_ref = sps.istft(view, nperseg=256, nfft=256)
+        for arr in (view, tview) if tview is not None else (view,):
+            _, x_got = msig.istft(arr, nperseg=256, nfft=256)
+            assert tuple(x_got.shape) == x_ref.shape
+            assert_close(x_got, x_ref)
+
+
 def test_stft_istft_roundtrip_ours(rng):
     x = make_sig(rng, (4096,))
     f, t, z = msig.stft(x, nperseg=256)
@@ -311,7 +368,18 @@ def test_memoised_setup_repeats(rng, fn):
             getattr(msig, fn)(xs, nperseg=256)
 
 
-def test_istft_plan_repeats_and_warns(rng):
+def test_istft_plan_repeats_and_warns(rng, monkeypatch):
+    from mlx_signal_b200 import spectral
+
+    built = []
+
+    class Counting(spectral._IstftPlan):
+        def __init__(self, *a, **k):
+            built.append(1)
+            super().__init__(*a, **k)
+
+    monkeypatch.setattr(spectral, "_IstftPlan", Counting)
+    spectral._ISTFT_PLANS.clear()
     for _ in range(3):
         x = make_sig(rng, (2, 5000))
         _, _, z = sps.stft(x.astype(np.float64), nperseg=256)
@@ -322,6 +390,9 @@ def test_istft_plan_repeats_and_warns(rng):
         assert_close(t, np.arange(x_ref.shape[-1], dtype=np.float64))
         assert_close(xr, x_ref)
         t.fill_(-1.0)
+    # one plan, built by the first call and found by the two repeats under the call's full key
+    assert len(built) == 1
+    assert [k[0] for k in spectral._ISTFT_PLANS] == ["istft"]
     # boxcar with no overlap and no boundary padding gaps -> NOLA fails on every call
     z = torch.from_numpy(sps.stft(make_sig(rng, (4096,)), window=("tukey", 0.0), nperseg=256,
                                   noverlap=0)[2].astype(np.complex64)).cuda()

@@ -95,6 +95,16 @@ def test_periodogram_matches_scipy(rng, case):
     assert_close(p, p_ref)
 
 
+def test_periodogram_array_window(rng):
+    x = make_sig(rng, (1024,))
+    w = sps.get_window("blackman", 1024)
+    _, p_ref = sps.periodogram(x.astype(np.float64), window=w)
+    _, p = msig.periodogram(x, window=w)
+    assert_close(p, p_ref)
+    _, p_t = msig.periodogram(x, window=torch.from_numpy(w).float().cuda())  # device window
+    assert_close(p_t, p_ref)
+
+
 def test_parseval_periodogram(rng):
     x = make_sig(rng, (4096,))
     fs = 10.0
