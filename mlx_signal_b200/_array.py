@@ -80,7 +80,7 @@ def to_device(x) -> torch.Tensor:
             arr = arr.astype(np.complex64)
         else:
             arr = arr.astype(np.float32)
-        return torch.from_numpy(np.ascontiguousarray(arr)).to(dev)
+        return torch.from_numpy(_c_order(arr)).to(dev)
     if x.dtype == np.float32 or x.dtype == np.complex64:
         arr = x
     elif x.dtype.kind == "f":
@@ -94,7 +94,13 @@ def to_device(x) -> torch.Tensor:
         arr = x.astype(np.float32)
     else:
         raise TypeError(f"unsupported input dtype: {x.dtype}")
-    return torch.from_numpy(np.ascontiguousarray(arr)).to(dev)
+    return torch.from_numpy(_c_order(arr)).to(dev)
+
+
+def _c_order(arr: np.ndarray) -> np.ndarray:
+    """C-contiguous view or copy that keeps 0-d arrays 0-d (np.ascontiguousarray returns at least
+    one dimension, which would turn a scalar input into shape (1,))."""
+    return np.asarray(arr, order="C")
 
 
 def to_numpy(x) -> np.ndarray:

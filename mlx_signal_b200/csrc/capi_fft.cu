@@ -69,15 +69,16 @@ template <int PASS, int LL>
 int launch_one(const CUtensorMap& map, Fft3Params p, int tiles, cudaStream_t s) {
   using CFG = Fft3Cfg<LL, fft3_log_e<LL>()>;
   auto k = &k_fft3_pass<LL, fft3_log_e<LL>(), PASS>;
+  constexpr size_t kSmem = CFG::smem(PASS);
   int sms = 0;
-  const int nb = resident_ctas(reinterpret_cast<const void*>(k), CFG::THREADS, CFG::SMEM, &sms);
+  const int nb = resident_ctas(reinterpret_cast<const void*>(k), CFG::THREADS, kSmem, &sms);
   if (nb <= 0) {
     set_error("no resident CTA for the fft3 pass (2^%d points per column)", LL);
     return SP_ERR_UNSUPPORTED;
   }
   p.ntiles = tiles;
   const int grid = tiles < nb * sms ? tiles : nb * sms;
-  k<<<grid, CFG::THREADS, CFG::SMEM, s>>>(map, p);
+  k<<<grid, CFG::THREADS, kSmem, s>>>(map, p);
   B2S_CHECK_CUDA(cudaGetLastError(), "fft3 pass launch");
   return SP_OK;
 }

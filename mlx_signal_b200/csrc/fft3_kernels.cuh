@@ -109,11 +109,26 @@ struct Fft3Cfg {
   static constexpr int L = PL::L;
   static constexpr int THREADS = kTileCols * PL::P;
   static constexpr int TILE_BYTES = L * kTileCols * 8;
-  // two tiles (1024-byte aligned for the swizzle) | exchange buffers | team twiddles |
-  // per-tile inter-pass twiddles (L + kTileCols double2) | 2 mbarriers
-  static constexpr size_t SMEM = 1024 + 2 * size_t(TILE_BYTES) +
-                                 size_t(kTileCols) * PL::BUF * 8 + size_t(PL::TW) * 8 +
-                                 size_t(L + kTileCols) * 16 + 16;
+  static constexpr int XBUF_BYTES = kTileCols * PL::BUF * 8;
+  // A slot holds a TMA tile and, once every team has its column in registers, the teams'
+  // exchange buffers: sized for the larger of the two, in whole 1024-byte swizzle units.
+  static constexpr int SLOT_BYTES =
+      ((TILE_BYTES > XBUF_BYTES ? TILE_BYTES : XBUF_BYTES) + 1023) / 1024 * 1024;
+  // alignment slack | two slots (1024-byte aligned for the swizzle) | team twiddles |
+  // per-tile inter-pass twiddles (L + kTileCols double2; passes 1 and 2) | 2 mbarriers
+  static constexpr size_t smem(int pass) {
+    return 1024 + 2 * size_t(SLOT_BYTES) + size_t(PL::TW) * 8 +
+           (pass == 3 ? 0 : size_t(L + kTileCols) * 16) + 16;
+  }
+  // CTAs per SM that the shared memory allows (228 KB per SM, 1 KB reserved per CTA, at most
+  // 2048 threads), asked of the register allocator for columns of 128 points and more; shorter
+  // columns (whose pass-2 code would spill under that bound) keep the default.
+  static constexpr int min_blocks(int pass) {
+    const int by_smem = int((228u * 1024u) / (smem(pass) + 1024));
+    const int by_threads = 2048 / THREADS;
+    const int b = by_smem < by_threads ? by_smem : by_threads;
+    return (L < 128 || b < 1) ? 1 : b;
+  }
 };
 
 // One pass of the three-pass FFT. PASS 1: tile rows m3 (L = R3), columns r; PASS 2: rows m2
@@ -133,7 +148,8 @@ __device__ __forceinline__ void fft3_tile_coords(int tile, int R1, int R2, int R
 }
 
 template <int LOG_L, int LOG_E, int PASS>
-__global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
+__global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
+                                  Fft3Cfg<LOG_L, LOG_E>::min_blocks(PASS))
     k_fft3_pass(const __grid_constant__ CUtensorMap src, Fft3Params pr) {
   using CFG = Fft3Cfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
@@ -142,11 +158,11 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
   // 1024-byte alignment for the swizzle, as an offset into the shared array (so every pointer
   // below stays in the shared address space: LDS/STS, not generic loads)
   const uint32_t pad = (1024u - (smem_u32(smraw) & 1023u)) & 1023u;
-  float2* tiles = reinterpret_cast<float2*>(smraw + pad);  // two tiles of L x kTileCols
-  float2* xbuf = tiles + 2 * L * kTileCols;
-  float2* tw = xbuf + kTileCols * PL::BUF;
+  constexpr int SLOT = CFG::SLOT_BYTES / 8;                 // float2 per slot
+  float2* tiles = reinterpret_cast<float2*>(smraw + pad);  // two slots
+  float2* tw = tiles + 2 * SLOT;
   double2* ttw = reinterpret_cast<double2*>(tw + PL::TW);  // this tile's inter-pass twiddles
-  uint64_t* bar = reinterpret_cast<uint64_t*>(ttw + L + kTileCols);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ttw + (PASS == 3 ? 0 : L + kTileCols));
   const int R1 = pr.R1, R2 = pr.R2, R3 = pr.R3;
   const int64_t N = pr.N;
   if (threadIdx.x == 0) {
@@ -159,7 +175,7 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
   auto issue = [&](int tl, int j) {  // thread 0: TMA load of tile tl into buffer j
     int cg_, slab_, b_;
     fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg_, &slab_, &b_);
-    float2* dst = tiles + j * (L * kTileCols);
+    float2* dst = tiles + j * SLOT;
     mbar_expect_tx(bar + j, uint32_t(CFG::TILE_BYTES));
     for (int r0 = 0; r0 < L; r0 += 256) {
       // box rows run along dim 2 for passes 1/2 ({2 col, slab, b L + row}) and along dim 1
@@ -213,13 +229,13 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
       }
       return;
     }
-    float2* tile = tiles + j * (L * kTileCols);
+    float2* tile = tiles + j * SLOT;
     int cg, slab, b;
     fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg, &slab, &b);
     const int col0 = cg * kTileCols;
     const int team = threadIdx.x / P, t = threadIdx.x - team * P;
     const unsigned mask = team_mask<P>();
-    float2* buf = xbuf + team * PL::BUF;
+    float2* buf = tile + team * PL::BUF;  // exchange buffer inside this tile's slot
     const int c = team;  // this team's column in the tile
     float2 v[E];
     static_for<0, E>([&](auto ec) {
@@ -229,6 +245,7 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
       if (PASS == 1 && pr.inverse) z.y = -z.y;
       v[e] = z;
     });
+    __syncthreads();  // every column is in registers: the slot becomes exchange space
     team_pass0<PL>(v);
     team_passes<PL>(v, buf, tw, t, mask);
     // output k = t + e*P of this column
@@ -268,7 +285,10 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS)
         *reinterpret_cast<float4*>(dst + row * row_stride + cp) = make_float4(a0.x, a0.y, a1.x, a1.y);
       }
     }
-    __syncthreads();  // buffer j is free for the load of tile it + 2
+    // The slot was written through the generic proxy (exchange, output staging); order those
+    // accesses before the TMA (async proxy) that refills it with tile it + 2.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();  // slot j is free for the load of tile it + 2
   }
 }
 
