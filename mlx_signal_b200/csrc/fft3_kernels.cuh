@@ -115,10 +115,10 @@ struct Fft3Cfg {
   static constexpr int SLOT_BYTES =
       ((TILE_BYTES > XBUF_BYTES ? TILE_BYTES : XBUF_BYTES) + 1023) / 1024 * 1024;
   // alignment slack | two slots (1024-byte aligned for the swizzle) | team twiddles |
-  // per-tile inter-pass twiddles (L + kTileCols double2; passes 1 and 2) | 2 mbarriers
+  // per-tile inter-pass twiddles (L + kTileCols float2; passes 1 and 2) | 2 mbarriers
   static constexpr size_t smem(int pass) {
     return 1024 + 2 * size_t(SLOT_BYTES) + size_t(PL::TW) * 8 +
-           (pass == 3 ? 0 : size_t(L + kTileCols) * 16) + 16;
+           (pass == 3 ? 0 : size_t(L + kTileCols) * 8) + 16;
   }
   // CTAs per SM that the shared memory allows (228 KB per SM, 1 KB reserved per CTA, at most
   // 2048 threads), asked of the register allocator for columns of 128 points and more; shorter
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
   constexpr int SLOT = CFG::SLOT_BYTES / 8;                 // float2 per slot
   float2* tiles = reinterpret_cast<float2*>(smraw + pad);  // two slots
   float2* tw = tiles + 2 * SLOT;
-  double2* ttw = reinterpret_cast<double2*>(tw + PL::TW);  // this tile's inter-pass twiddles
+  float2* ttw = tw + PL::TW;  // this tile's inter-pass twiddles
   uint64_t* bar = reinterpret_cast<uint64_t*>(ttw + (PASS == 3 ? 0 : L + kTileCols));
   const int R1 = pr.R1, R2 = pr.R2, R3 = pr.R3;
   const int64_t N = pr.N;
@@ -198,25 +198,26 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
     if (threadIdx.x == 0 && nxt < pr.ntiles) issue(nxt, j ^ 1);
     // This tile's inter-pass twiddles, computed while its copy is in flight (the previous
     // tile's readers finished at the last barrier; the wait below publishes them). Each is an
-    // independent FP64 sincospi of an exactly reduced integer phase:
-    //   pass 1: W_N^(R1 m2 km3) (times 1/N for the inverse), one per output row km3, rounded
-    //           once to FP32 and shared by every column of the tile;
-    //   pass 2: W_N^(r km2 R3) per row km2 and W_N^(r km3) per column km3, kept in FP64 and
-    //           multiplied per element (rounded once).
+    // independent FP64 sincospi of an exactly reduced integer phase, rounded once to FP32:
+    //   pass 1: W_N^(R1 m2 km3) (times 1/N for the inverse), one per output row km3, shared by
+    //           every column of the tile;
+    //   pass 2: W_N^(r km2 R3) per row km2 and W_N^(r km3) per column km3, multiplied per
+    //           element in FP32 (about one ulp more than a product rounded once; no FP64 work
+    //           per element).
     if constexpr (PASS != 3) {
       int cg_, slab_, b_;
       fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg_, &slab_, &b_);
       if constexpr (PASS == 1) {
         const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
-        float2* t1 = reinterpret_cast<float2*>(ttw);
         for (int i = threadIdx.x; i < L; i += blockDim.x) {
           const double2 w = w_exact(int64_t(R1) * slab_ * i, N);
-          t1[i] = make_float2(float(w.x * sc), float(w.y * sc));
+          ttw[i] = make_float2(float(w.x * sc), float(w.y * sc));
         }
       } else {
         for (int i = threadIdx.x; i < L + kTileCols; i += blockDim.x) {
-          ttw[i] = i < L ? w_exact(int64_t(slab_) * i * R3, N)
-                         : w_exact(int64_t(slab_) * (cg_ * kTileCols + (i - L)), N);
+          const double2 w = i < L ? w_exact(int64_t(slab_) * i * R3, N)
+                                  : w_exact(int64_t(slab_) * (cg_ * kTileCols + (i - L)), N);
+          ttw[i] = make_float2(float(w.x), float(w.y));
         }
       }
     }
@@ -252,19 +253,15 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
     if constexpr (PASS == 1) {
       // twiddle W_N^(R1 m2 km3) of output row km3 = t + e P, from the tile table
       const int m2 = slab, r = col0 + c;
-      const float2* t1 = reinterpret_cast<const float2*>(ttw);
       float2* dst = pr.out + int64_t(b) * N + (int64_t(m2) * R1 + r) * R3;
 #pragma unroll
-      for (int e = 0; e < E; ++e) dst[t + e * P] = cmul(v[e], t1[t + e * P]);
+      for (int e = 0; e < E; ++e) dst[t + e * P] = cmul(v[e], ttw[t + e * P]);
     } else {
       if constexpr (PASS == 2) {
         // twiddle W_N^(r (km2 R3 + km3)) = W_N^(r km2 R3) W_N^(r km3), km2 = t + e P
-        const double2 wc = ttw[L + c];
+        const float2 wc = ttw[L + c];
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const double2 w = zmul(ttw[t + e * P], wc);
-          v[e] = cmul(v[e], make_float2(float(w.x), float(w.y)));
-        }
+        for (int e = 0; e < E; ++e) v[e] = cmul(v[e], cmul(ttw[t + e * P], wc));
       }
       __syncthreads();  // every team has read its column: the tile can be overwritten
   #pragma unroll
