@@ -15,9 +15,10 @@
 //    (cp.async.bulk.tensor, 128B swizzle, mbarrier completion, no multicast), so the strided
 //    column walk of the reference's per-thread gather becomes one coalesced bulk transfer;
 //  * each tile column is an L-point team FFT in registers (the spectral kernels' engine);
-//  * inter-pass twiddles are generated per element in FP64 from the exact integer phase
-//    (sincospi of one anchor per lane, then an FP64 recurrence over the lane's E outputs) and
-//    rounded to FP32 once -- no twiddle table in memory;
+//  * inter-pass twiddles come from per-tile shared-memory tables filled while the tile's copy
+//    is in flight, each entry an FP64 sincospi of the exactly reduced integer phase rounded to
+//    FP32 once (pass 1: one per output row; pass 2: one per row and one per column, multiplied
+//    per element in FP32) -- no twiddle table in global memory;
 //  * the inverse transform is conj(FFT(conj(x))) / N with 1/N folded into pass 1.
 // Every mbarrier wait is bounded; on timeout the CTA records SP_ERR_TIMEOUT in the error word,
 // waits (bounded) for its own copy and returns without touching the data.
