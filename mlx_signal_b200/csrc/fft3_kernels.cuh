@@ -308,6 +308,15 @@ __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restric
   const int64_t k0 = (blockIdx.x - b * per_row) * (kUntB * kUntT) + threadIdx.x;
   const float2* z = Z + b * m;
   float2* x = X + b * ldx;
+  // Every read of the thread first, so that its 2 kUntT loads are in flight together: the
+  // kernel waits on the latency of these (L2-resident) reads, not on bandwidth.
+  float2 zks[kUntT], zms[kUntT];
+#pragma unroll
+  for (int j = 0; j < kUntT; ++j) {
+    const int64_t k = k0 + int64_t(j) * kUntB;
+    zks[j] = k < half ? z[k] : make_float2(0.f, 0.f);
+    zms[j] = (k < half && k != 0) ? z[m - k] : make_float2(0.f, 0.f);
+  }
   double sn, cs;
   sincospi(-double(k0) / double(m), &sn, &cs);
   double2 w = make_double2(cs, sn);
@@ -316,11 +325,11 @@ __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restric
     const int64_t k = k0 + int64_t(j) * kUntB;
     if (k < half) {
       if (k == 0) {
-        const float2 z0 = z[0];
+        const float2 z0 = zks[j];
         x[0] = make_float2(z0.x + z0.y, 0.f);
         x[m] = make_float2(z0.x - z0.y, 0.f);
       } else {
-        const float2 zk = z[k], zm = z[m - k];
+        const float2 zk = zks[j], zm = zms[j];
         const float2 wf = make_float2(float(w.x), float(w.y));
         // X_{m-k} shares zk, zm: ze' = conj(ze), zo' = -conj(zo), w_{m-k} = -conj(w_k)
         const float2 ze = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
@@ -356,6 +365,13 @@ __global__ void __launch_bounds__(kUntB) k_irfft_pretwist(const float2* __restri
     if (j == 0 || j == m) v.y = 0.f;
     return v;
   };
+  float2 xks[kUntT], xms[kUntT];  // every read first, as in the untangle
+#pragma unroll
+  for (int j = 0; j < kUntT; ++j) {
+    const int64_t k = k0 + int64_t(j) * kUntB;
+    xks[j] = k < half ? get(k) : make_float2(0.f, 0.f);
+    xms[j] = k < half ? get(m - k) : make_float2(0.f, 0.f);
+  }
   double sn, cs;
   sincospi(-double(k0) / double(m), &sn, &cs);
   double2 w = make_double2(cs, sn);
@@ -363,7 +379,7 @@ __global__ void __launch_bounds__(kUntB) k_irfft_pretwist(const float2* __restri
   for (int j = 0; j < kUntT; ++j) {
     const int64_t k = k0 + int64_t(j) * kUntB;
     if (k < half) {
-      const float2 xk = get(k), xm = get(m - k);
+      const float2 xk = xks[j], xm = xms[j];
       const float c = float(w.x), sf = float(w.y);
       const float2 wc = make_float2(c, -sf);  // conj(w_k)
       const float2 e1 = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y - xm.y));

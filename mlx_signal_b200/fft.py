@@ -7,7 +7,7 @@ complex length (n for fft/ifft, n/2 for rfft/irfft) is a power of two in
 [2^KERNEL_MIN_LOG2, 2^26] run the three-pass TMA-staged kernels (the C-ABI takes every power of
 two from 2^12); other lengths run cuFFT through torch.fft (the composed GPU path; the reference
 uses MLX's own FFT there). The default threshold 2^20 is where the kernels match cuFFT (measured:
-rfft 2^23 68 vs 66 us, 2^24 125 vs 131 us, 8 x 2^23 416 vs 459 us; shorter or batched-short
+rfft 2^23 68 vs 66 us, 2^24 120 vs 132 us, 8 x 2^23 408 vs 459 us; shorter or batched-short
 transforms are faster in cuFFT). numpy.fft semantics for `n` (zero-pad or truncate) and `axis`.
 """
 
