@@ -170,6 +170,34 @@ def test_grouped_spectral_means_match_scipy(rng, nperseg, detrend):
     assert_close(co, co_ref, rtol=1e-3)
 
 
+def test_grouped_spectral_reduces_peak_memory(rng):
+    """Segment sums accumulate in the kernels: no per-frame spectra are materialised (the
+    reference's tests/test_spectral.py:233-263 bounds, 64 x 2^19, nperseg 1024, where per-frame
+    coherence spectra would take ~512 MiB)."""
+    x = torch.from_numpy(rng.standard_normal((64, 1 << 19)).astype(np.float32)).cuda()
+    y = torch.from_numpy(rng.standard_normal((64, 1 << 19)).astype(np.float32)).cuda()
+    msig.welch(x, nperseg=1024)
+    msig.coherence(x, y, nperseg=1024)
+    msig.csd(x, y, nperseg=1024)
+    torch.cuda.synchronize()
+
+    def peak_mib(fn):
+        base = torch.cuda.memory_allocated()
+        torch.cuda.reset_peak_memory_stats()
+        out = fn()
+        torch.cuda.synchronize()
+        peak = (torch.cuda.max_memory_allocated() - base) / (1 << 20)
+        del out
+        return peak
+
+    welch_mib = peak_mib(lambda: msig.welch(x, nperseg=1024))
+    coh_mib = peak_mib(lambda: msig.coherence(x, y, nperseg=1024))
+    csd_mib = peak_mib(lambda: msig.csd(x, y, nperseg=1024))
+    assert welch_mib < 16.0, f"welch peak memory too high: {welch_mib:.1f} MiB"
+    assert coh_mib < 64.0, f"coherence peak memory too high: {coh_mib:.1f} MiB"
+    assert csd_mib < 64.0, f"csd peak memory too high: {csd_mib:.1f} MiB"
+
+
 def test_grouped_single_group_and_nonlast_axis(rng):
     x_many = make_sig(rng, (2048, 320))
     y_many = (0.5 * x_many + 0.5 * make_sig(rng, (2048, 320))).astype(np.float32)
