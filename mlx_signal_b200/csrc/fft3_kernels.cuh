@@ -155,6 +155,10 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
   using CFG = Fft3Cfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
   constexpr int L = PL::L, E = PL::E, P = PL::P;
+  static_assert(CFG::SLOT_BYTES >= CFG::TILE_BYTES && CFG::SLOT_BYTES >= CFG::XBUF_BYTES &&
+                    CFG::SLOT_BYTES % 1024 == 0,
+                "a slot holds the TMA tile and every team's exchange buffer, swizzle-aligned");
+  static_assert(CFG::smem(PASS) <= 227u * 1024u, "pass exceeds the shared memory of one CTA");
   extern __shared__ __align__(16) unsigned char smraw[];
   // 1024-byte alignment for the swizzle, as an offset into the shared array (so every pointer
   // below stays in the shared address space: LDS/STS, not generic loads)
