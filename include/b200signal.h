@@ -119,13 +119,16 @@ SP_API int sp_welch_spectral_bins(int nfft);
  * sp_welch_f32 without a workspace argument, for callers that cannot allocate device memory
  * (plugin hosts that only receive input/output pointers, latency-critical loops that must not
  * call cudaMalloc after start-up). No counterpart in the reference: it is an addition of this
- * library. The partial sums live in a fixed 16 MiB static device array that every GPU loading
- * the library holds until exit; shapes needing more scratch than that return SP_ERR_WORKSPACE
+ * library. The partial sums live in a fixed 16 MiB static device array, held on each device from
+ * the first use of the library's spectral-mean kernels there (modules load lazily by default)
+ * until the process exits; shapes needing more scratch than that return SP_ERR_WORKSPACE
  * (sp_mean_workspace_size(0, ...) gives the need). It calls no cudaMalloc/cudaFree. The first
- * call on a device resolves the array's device address (cudaGetSymbolAddress) and should come
- * before any stream capture. All calls share the one array: calls that overlap on the GPU (for
- * example on two streams at once) race and must be serialised by the caller. Nothing from a
- * previous call is read: every partial sum a call reads is written by that call first.
+ * call on a device resolves the array's device address (cudaGetSymbolAddress, with that device
+ * current) and should come before any stream capture; the address is cached per device and
+ * resolved again when the device's context changes (after a cudaDeviceReset). All calls share
+ * the one array: calls that overlap on the GPU (for example on two streams at once) race and
+ * must be serialised by the caller. Nothing from a previous call is read: every partial sum a
+ * call reads is written by that call first.
  */
 SP_API int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld,
                                 const float* win, int nperseg, int nfft, int hop, int detrend,
@@ -283,6 +286,16 @@ SP_API int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int ba
 /* Byte offset of the int error word inside a long-transform workspace (0 = ok, SP_ERR_TIMEOUT if
  * a tile copy wait gave up); read it after synchronising the stream. */
 SP_API int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_t* offset);
+
+/*
+ * Poll limit of the bounded wait each long-transform CTA makes for a tile's TMA copy (process
+ * wide, read at every launch; 0xffffffff restores the default of 2^22 polls). A wait that runs
+ * out records SP_ERR_TIMEOUT in the error word, drains its own copies (bounded by the default
+ * limit) and returns; the transform's output is then undefined. A host watchdog test sets it to
+ * 0 to make every wait run out. Returns the previous limit. No counterpart in the reference
+ * (its Metal kernels have no device-side waits, _fourstep_metal.py:58-185).
+ */
+SP_API uint32_t sp_fft_set_wait_limit(uint32_t polls);
 
 /*
  * FFT convolution of each of `rows` real rows x (n1 samples, row stride ld_x) with one real filter

@@ -13,7 +13,7 @@ import warnings
 import numpy as np
 import torch
 
-from ._config import DowncastWarning, _config
+from ._config import DowncastWarning, get_config
 
 
 def device() -> torch.device:
@@ -23,13 +23,14 @@ def device() -> torch.device:
 
 
 def _downcast_notice(src: str) -> None:
-    if _config.float64 == "strict":
+    cfg = get_config()
+    if cfg.float64 == "strict":
         raise TypeError(
             f"{src} input is not supported with float64='strict' (the kernels compute in "
             "float32). Cast to float32/complex64, or set "
             "mlx_signal_b200.set_config(float64='downcast')."
         )
-    if _config.warn_on_downcast:
+    if cfg.warn_on_downcast:
         warnings.warn(
             f"{src} input downcast to 32-bit (the CUDA kernels compute in float32); "
             "results are float32-accurate",

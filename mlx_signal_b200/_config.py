@@ -1,11 +1,16 @@
 """Global configuration: dtype policy and warnings.
 
-Mirrors the reference's ``Config`` / ``set_config`` / ``config_context``
-(src/mlx_signal_processing/_config.py:42-91) for the options that change results. The
-reference's size-based dispatch to scipy.signal (``dispatch``/``gpu_min_size``,
-_config.py:94-100) has no counterpart: every call runs on the GPU, there is no CPU path.
-``dispatch`` is still accepted for source compatibility; only "auto" and "cuda" (alias "mlx")
-are valid, and both mean the CUDA kernels.
+The option names and exception types follow the reference's ``Config`` / ``set_config`` /
+``config_context`` (src/mlx_signal_processing/_config.py:42-91) so that code written against it
+keeps working. The reference's size-based dispatch to scipy.signal (``dispatch``/
+``gpu_min_size``, _config.py:94-100) has no counterpart: every call runs on the GPU and there is
+no CPU path. ``dispatch`` is still accepted for source compatibility; only "auto" and "cuda"
+(alias "mlx") are valid, and both mean the CUDA kernels.
+
+Design: the active configuration is one immutable ``Config`` value held in a module slot.
+``set_config`` builds the whole replacement value, checks every field of it against the option
+table below, and only then swaps it in, so a rejected call leaves nothing half-applied;
+``config_context`` restores the exact value object it found on entry.
 """
 
 from __future__ import annotations
@@ -13,6 +18,7 @@ from __future__ import annotations
 import contextlib
 import dataclasses
 import warnings
+from typing import Any, Callable
 
 __all__ = [
     "Config",
@@ -23,9 +29,6 @@ __all__ = [
     "set_config",
 ]
 
-_DISPATCH_MODES = ("auto", "cuda", "mlx")
-_FLOAT64_MODES = ("downcast", "strict")
-
 
 class FallbackWarning(UserWarning):
     """A call used the composed (library FFT) GPU path instead of a fused kernel."""
@@ -35,57 +38,84 @@ class DowncastWarning(UserWarning):
     """float64/complex128 input was downcast to float32/complex64."""
 
 
-@dataclasses.dataclass
+@dataclasses.dataclass(frozen=True)
 class Config:
     dispatch: str = "auto"
     float64: str = "downcast"  # or "strict" (raise on float64 input)
     warn_on_downcast: bool = True
-    warn_on_fallback: bool = False
+    # loud by default: a shape that leaves the fused kernels says so
+    warn_on_fallback: bool = True
     #: byte budget of device-resident constant caches (windows, twiddles)
     cache_bytes: int = 64 << 20
 
 
-_config = Config()
+def _one_of(*allowed: str, note: str = "") -> Callable[[str, Any], str | None]:
+    def check(name: str, value: Any) -> str | None:
+        if value in allowed:
+            return None
+        return f"{name} must be one of {allowed}{note}"
+
+    return check
+
+
+def _flag(name: str, value: Any) -> str | None:
+    return None if isinstance(value, bool) else f"{name} must be True or False"
+
+
+def _byte_count(name: str, value: Any) -> str | None:
+    ok = isinstance(value, int) and not isinstance(value, bool) and value >= 0
+    return None if ok else f"{name} must be a non-negative integer"
+
+
+# option -> validator returning an error message (or None when the value is acceptable)
+_CHECKS: dict[str, Callable[[str, Any], str | None]] = {
+    "dispatch": _one_of("auto", "cuda", "mlx", note=" (this build has no CPU/scipy path)"),
+    "float64": _one_of("downcast", "strict"),
+    "warn_on_downcast": _flag,
+    "warn_on_fallback": _flag,
+    "cache_bytes": _byte_count,
+}
+
+_active: Config = Config()
 
 
 def get_config() -> Config:
-    """Return a copy of the current global configuration."""
-    return dataclasses.replace(_config)
+    """The configuration in force (an immutable value; change it with ``set_config``)."""
+    return _active
 
 
 def set_config(**kwargs) -> None:
-    """Update configuration options (validated before anything changes)."""
-    for key in kwargs:
-        if not hasattr(_config, key):
-            raise TypeError(f"unknown config option {key!r}")
-    if kwargs.get("dispatch", _config.dispatch) not in _DISPATCH_MODES:
-        raise ValueError(
-            f"dispatch must be one of {_DISPATCH_MODES} (this build has no CPU/scipy path)"
-        )
-    if kwargs.get("float64", _config.float64) not in _FLOAT64_MODES:
-        raise ValueError(f"float64 must be one of {_FLOAT64_MODES}")
-    size = kwargs.get("cache_bytes", _config.cache_bytes)
-    if not isinstance(size, int) or isinstance(size, bool) or size < 0:
-        raise ValueError("cache_bytes must be a non-negative integer")
-    for key, value in kwargs.items():
-        setattr(_config, key, value)
+    """Replace the named options. Unknown names raise TypeError and bad values ValueError,
+    before any option changes."""
+    global _active
+    unknown = sorted(set(kwargs) - set(_CHECKS))
+    if unknown:
+        raise TypeError(f"unknown config option {unknown[0]!r}")
+    candidate = dataclasses.replace(_active, **kwargs)
+    for name, check in _CHECKS.items():
+        problem = check(name, getattr(candidate, name))
+        if problem is not None:
+            raise ValueError(problem)
+    _active = candidate
 
 
 @contextlib.contextmanager
 def config_context(**kwargs):
-    """Temporarily override configuration options within a ``with`` block."""
-    old = dataclasses.asdict(_config)
+    """Apply ``set_config(**kwargs)`` inside a ``with`` block and put the previous
+    configuration back on exit (also when the block raises)."""
+    global _active
+    saved = _active
     try:
         set_config(**kwargs)
-        yield
+        yield _active
     finally:
-        _config.__dict__.update(old)
+        _active = saved
 
 
 def composed_path_notice(func_name: str, reason: str) -> None:
-    """Record that a call runs on the composed GPU path (cuFFT-backed) rather than a fused
-    kernel. Silent unless ``warn_on_fallback`` is set."""
-    if _config.warn_on_fallback:
+    """Emit a FallbackWarning (unless ``warn_on_fallback`` is off) for a call that runs on the
+    composed GPU path (strided frames + torch ops + cuFFT) instead of a fused kernel."""
+    if _active.warn_on_fallback:
         warnings.warn(
             f"mlx_signal_b200.{func_name}: {reason}; using the composed GPU path",
             FallbackWarning,

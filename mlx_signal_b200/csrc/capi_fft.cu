@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "capi_common.h"
@@ -11,6 +12,9 @@ namespace b2s {
 namespace {
 
 constexpr int kMinLogN = 12, kMaxLogN = 26;
+
+// poll limit of the per-tile copy waits (sp_fft_set_wait_limit)
+std::atomic<uint32_t> g_wait_polls{kMbarSpinLimit};
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -114,6 +118,7 @@ int fft3(const float2* in, float2* s1, float2* s2, float2* out, int batch, int e
   p.inverse = inverse;
   p.err = err;
   p.ntiles = 0;
+  p.wait_polls = g_wait_polls.load(std::memory_order_relaxed);
   const int l3 = ilog2_exact(R3), l2 = ilog2_exact(R2), l1 = ilog2_exact(R1);
   CUtensorMap m1, m2, m3;
   int st;
@@ -265,6 +270,10 @@ int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, in
   B2S_CHECK_CUDA(cudaGetLastError(), "irfft pretwist launch");
   // Y (in s2) -> S1 (s1) -> S2 (s2, Y already consumed by pass 1) -> x
   return fft3(s2, s1, s2, reinterpret_cast<float2*>(x), batch, e, 1, err, s);
+}
+
+uint32_t sp_fft_set_wait_limit(uint32_t polls) {
+  return b2s::g_wait_polls.exchange(polls == 0xffffffffu ? b2s::kMbarSpinLimit : polls);
 }
 
 int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_t* offset) {

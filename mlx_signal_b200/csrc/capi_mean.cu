@@ -1,4 +1,6 @@
 // C-ABI: segment-mean spectral estimates (welch / csd / coherence).
+#include <cuda.h>
+
 #include <mutex>
 #include <utility>
 
@@ -276,19 +278,40 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
 // time: plugin hosts that only hand over input/output pointers owned by another framework, and
 // latency-critical loops that must not take cudaMalloc's implicit device synchronisation or
 // grow their footprint after start-up. For them the partial-sum workspace lives in this
-// file-scope array. It is created when the library's module is loaded on a device and stays
-// allocated on every GPU that loads the library until the process exits.
+// file-scope array. A device holds it from the first use of this file's kernels there (the
+// module is loaded lazily by default) until the process exits.
 // ---------------------------------------------------------------------------------------------
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+struct NoAllocSlot {
+  CUcontext ctx = nullptr;  // context the address was resolved in
+  void* addr = nullptr;
+};
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
+
+// cuCtxGetCurrent through the runtime's driver entry-point query (no link-time libcuda
+// dependency, so the library still loads on machines without a driver).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
 
 // Device address of the scratch array on the current device. In host code the array's name is
-// only a host-side stand-in, so the address comes from cudaGetSymbolAddress, once per device
-// (with that device current), and is cached.
+// only a host-side stand-in, so the address comes from cudaGetSymbolAddress, resolved with the
+// device current and cached per device together with the context it was resolved in: after a
+// cudaDeviceReset the device gets a new primary context (and a freshly loaded module), so the
+// cached address is resolved again instead of being reused.
 int noalloc_scratch(void** out) {
   int dev = 0;
   B2S_CHECK_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
@@ -297,13 +320,20 @@ int noalloc_scratch(void** out) {
               kNoAllocMaxDevices);
     return SP_ERR_ARG;
   }
+  // the plan query before this call (occupancy) has made the device's context current
+  CUcontext ctx = nullptr;
+  const CtxGetCurrentFn get = ctx_get_current();
+  if (get == nullptr || get(&ctx) != CUDA_SUCCESS) ctx = nullptr;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (g_noalloc_addr[dev] == nullptr) {
+  NoAllocSlot& slot = g_noalloc_slot[dev];
+  // without a context handle to compare, resolve the address on every call
+  if (slot.addr == nullptr || ctx == nullptr || slot.ctx != ctx) {
     void* p = nullptr;
     B2S_CHECK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
-    g_noalloc_addr[dev] = p;
+    slot.ctx = ctx;
+    slot.addr = p;
   }
-  *out = g_noalloc_addr[dev];
+  *out = slot.addr;
   return SP_OK;
 }
 

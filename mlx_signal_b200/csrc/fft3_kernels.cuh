@@ -21,7 +21,9 @@
 //    per element in FP32) -- no twiddle table in global memory;
 //  * the inverse transform is conj(FFT(conj(x))) / N with 1/N folded into pass 1.
 // Every mbarrier wait is bounded; on timeout the CTA records SP_ERR_TIMEOUT in the error word,
-// waits (bounded) for its own copy and returns without touching the data.
+// waits (bounded) for its own copies and returns without touching the data. The limit of the
+// wait for each tile is a launch parameter (sp_fft_set_wait_limit), so a host watchdog test can
+// make it run out.
 #pragma once
 
 #include <cuda.h>
@@ -42,6 +44,7 @@ struct Fft3Params {
   int inverse;         // 1: conj on load (pass 1) and on store (pass 3), scale 1/N in pass 1
   int* err;            // device error word (0 = ok)
   int ntiles;          // tiles of this pass (a persistent CTA walks tile, tile + gridDim.x, ...)
+  uint32_t wait_polls; // poll limit of the wait for each tile's copy (kMbarSpinLimit by default)
 };
 
 constexpr int kTileCols = 16;                  // columns per tile: 16 complex = 128 B rows
@@ -61,10 +64,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// true when the phase with parity `parity` has completed; bounded polling
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// true when the phase with parity `parity` has completed; at most `polls` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t polls = kMbarSpinLimit) {
   uint32_t done = 0;
-  for (uint32_t it = 0; it < kMbarSpinLimit; ++it) {
+  for (uint32_t it = 0; it < polls; ++it) {
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
         " selp.u32 %0, 1, 0, p;\n}\n"
@@ -226,11 +230,13 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
         }
       }
     }
-    const bool ok = __syncthreads_and(mbar_wait(bar + j, par) ? 1 : 0) != 0;
+    const bool ok = __syncthreads_and(mbar_wait(bar + j, par, pr.wait_polls) ? 1 : 0) != 0;
     if (!ok) {
       if (threadIdx.x == 0) {
         atomicExch(pr.err, SP_ERR_TIMEOUT);
-        (void)mbar_wait(bar + j, par);  // bounded second waits for the copies still in flight
+        // bounded second waits (full limit) for the copies still in flight, so that no TMA
+        // write lands in this CTA's shared memory after it exits
+        (void)mbar_wait(bar + j, par);
         if (nxt < pr.ntiles) (void)mbar_wait(bar + (j ^ 1), uint32_t((it + 1) >> 1) & 1u);
       }
       return;

@@ -21,7 +21,7 @@ from . import _lib
 from ._array import stream_handle, to_device
 from ._config import composed_path_notice
 
-__all__ = ["fft", "ifft", "irfft", "rfft"]
+__all__ = ["DeviceWaitTimeout", "device_status", "fft", "ifft", "irfft", "rfft"]
 
 MIN_LOG2, MAX_LOG2 = 12, 26   # lengths the C-ABI accepts
 KERNEL_MIN_LOG2 = 20          # lengths the Python API routes to the kernels
@@ -31,6 +31,14 @@ def _pow2_in_range(m: int) -> bool:
     """True when a complex transform of length m runs on the three-pass kernels."""
     lo = max(MIN_LOG2, KERNEL_MIN_LOG2)
     return m >= 1 and (m & (m - 1)) == 0 and lo <= m.bit_length() - 1 <= MAX_LOG2
+
+
+def _notice_long(func_name: str, m: int) -> None:
+    """cuFFT is this module's designed path for complex lengths below 2^KERNEL_MIN_LOG2 (it is
+    faster there); a long transform the three-pass kernels cannot take (not a power of two, or
+    beyond 2^26) is a fallback and says so."""
+    if m >= (1 << KERNEL_MIN_LOG2):
+        composed_path_notice(func_name, "length outside the three-pass kernels")
 
 
 def _last(t: torch.Tensor, axis: int) -> torch.Tensor:
@@ -58,8 +66,75 @@ def _workspace(n_complex: int, batch: int, dev) -> torch.Tensor:
     return torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
 
 
+class DeviceWaitTimeout(_lib.KernelError):
+    """A long transform's bounded device wait ran out (SP_ERR_TIMEOUT in its error word): its
+    output is undefined."""
+
+
+class _StatusWatch:
+    """Host watchdog for the long transforms' device error words. After each launch the word is
+    copied (stream-ordered, no synchronisation) into a slot of a pinned ring with an event; a
+    later call, or `device_status()`, reads the slots whose events completed and raises
+    DeviceWaitTimeout for a non-zero word."""
+
+    SLOTS = 64
+
+    def __init__(self):
+        self.host = None
+        self.live: list = []  # (slot, event, what)
+        self.next = 0
+
+    def record(self, ws: torch.Tensor, n_complex: int, batch: int, what: str) -> None:
+        if self.host is None:
+            self.host = torch.zeros(self.SLOTS, dtype=torch.int32, pin_memory=True)
+        import ctypes
+
+        off = ctypes.c_int64(0)
+        _lib.check(_lib.load().sp_fft_error_word(ws.data_ptr(), n_complex, batch,
+                                                 ctypes.byref(off)), "sp_fft_error_word")
+        if len(self.live) >= self.SLOTS:  # ring full: the oldest slot must be read first
+            self.poll(wait_oldest=True)
+        slot = self.next
+        self.next = (self.next + 1) % self.SLOTS
+        word = ws[off.value : off.value + 4].view(torch.int32)
+        self.host[slot : slot + 1].copy_(word, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self.live.append((slot, ev, what))
+
+    def poll(self, wait_oldest: bool = False, wait_all: bool = False) -> int:
+        status = 0
+        keep = []
+        for i, (slot, ev, what) in enumerate(self.live):
+            if wait_all or (wait_oldest and i == 0):
+                ev.synchronize()
+            if not ev.query():
+                keep.append((slot, ev, what))
+                continue
+            word = int(self.host[slot])
+            if word != 0 and status == 0:
+                status = word
+                failed = what
+        self.live = keep
+        if status != 0:
+            text = ("a bounded device wait ran out; the output of that transform is undefined"
+                    if status == _lib.SP_ERR_TIMEOUT else "device error word set")
+            raise DeviceWaitTimeout(failed, status, text)
+        return status
+
+
+_watch = _StatusWatch()
+
+
+def device_status() -> int:
+    """Wait for every long transform issued so far and return 0, or raise DeviceWaitTimeout if
+    one of them recorded a device-side wait timeout."""
+    return _watch.poll(wait_all=True)
+
+
 def rfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
     """One-sided FFT of real input (complex64 out, n//2+1 bins)."""
+    _watch.poll()
     x = to_device(a)
     if x.is_complex():
         x = x.real
@@ -75,13 +150,15 @@ def rfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
         _lib.check(_lib.load().sp_rfft_c64(xr.data_ptr(), out.data_ptr(), rows, n, n // 2 + 1,
                                            ws.data_ptr(), ws.numel(), stream_handle()),
                    "sp_rfft_c64")
+        _watch.record(ws, n // 2, rows, "rfft")
         return _back(out.reshape(batch + (n // 2 + 1,)), axis)
-    composed_path_notice("rfft", "length outside the three-pass kernels")
+    _notice_long("rfft", n // 2)
     return _back(torch.fft.rfft(x, n=n, dim=-1), axis)
 
 
 def irfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
     """Inverse of rfft: real float32 output of length n (default 2*(bins-1))."""
+    _watch.poll()
     X = to_device(a)
     if not X.is_complex():
         X = X.to(torch.complex64)
@@ -97,12 +174,14 @@ def irfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
         _lib.check(_lib.load().sp_irfft_f32(Xr.data_ptr(), nb, nb, out.data_ptr(), rows, n,
                                             ws.data_ptr(), ws.numel(), stream_handle()),
                    "sp_irfft_f32")
+        _watch.record(ws, n // 2, rows, "irfft")
         return _back(out.reshape(batch + (n,)), axis)
-    composed_path_notice("irfft", "length outside the three-pass kernels")
+    _notice_long("irfft", n // 2)
     return _back(torch.fft.irfft(X, n=n, dim=-1), axis)
 
 
 def _cfft(a, n, axis, inverse: bool) -> torch.Tensor:
+    _watch.poll()
     z = to_device(a)
     if not z.is_complex():
         z = z.to(torch.complex64)
@@ -118,8 +197,9 @@ def _cfft(a, n, axis, inverse: bool) -> torch.Tensor:
         _lib.check(_lib.load().sp_fft_c64(zr.data_ptr(), out.data_ptr(), rows, n, int(inverse),
                                           ws.data_ptr(), ws.numel(), stream_handle()),
                    "sp_fft_c64")
+        _watch.record(ws, n, rows, "ifft" if inverse else "fft")
         return _back(out.reshape(batch + (n,)), axis)
-    composed_path_notice("fft", "length outside the three-pass kernels")
+    _notice_long("ifft" if inverse else "fft", n)
     f = torch.fft.ifft if inverse else torch.fft.fft
     return _back(f(z, n=n, dim=-1), axis)
 

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 from scipy.signal import get_window as _sp_get_window
 
-from ._config import _config
+from ._config import get_config
 
 __all__ = ["get_window"]
 
@@ -77,7 +77,7 @@ class ByteBudgetCache:
         return len(self._entries)
 
 
-DEVICE_CONSTANTS = ByteBudgetCache(_config.cache_bytes)
+DEVICE_CONSTANTS = ByteBudgetCache(get_config().cache_bytes)
 
 
 def device_vector(values: np.ndarray, dtype=torch.float32) -> torch.Tensor:

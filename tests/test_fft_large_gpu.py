@@ -110,6 +110,51 @@ def test_error_word_clear_after_transform(rng):
     assert int(ws[off.value : off.value + 4].view(torch.int32).item()) == 0
 
 
+def test_bounded_wait_runs_out_and_reports_timeout(rng, monkeypatch):
+    """Failure detection without a fault: with a poll limit of 0 every tile-copy wait runs out,
+    each CTA records SP_ERR_TIMEOUT in the error word, drains its own copies (bounded) and
+    returns; the host reads the word through the C-ABI and through the Python watchdog, and the
+    next transform with the default limit is clean and correct."""
+    from mlx_signal_b200 import _lib
+
+    lib = _lib.load()
+    n = 1 << 16
+    x = torch.from_numpy((rng.standard_normal(n) + 1j * rng.standard_normal(n))
+                         .astype(np.complex64)).cuda()
+    out = torch.empty_like(x)
+    ws = torch.zeros(int(lib.sp_fft_workspace_size(n, 1)), dtype=torch.uint8, device="cuda")
+    off = ctypes.c_int64(0)
+    assert lib.sp_fft_error_word(ws.data_ptr(), n, 1, ctypes.byref(off)) == 0
+    stream = torch.cuda.current_stream().cuda_stream
+    prev = lib.sp_fft_set_wait_limit(0)
+    try:
+        assert lib.sp_fft_c64(x.data_ptr(), out.data_ptr(), 1, n, 0, ws.data_ptr(), ws.numel(),
+                              stream) == 0
+        torch.cuda.synchronize()
+        assert int(ws[off.value : off.value + 4].view(torch.int32).item()) == _lib.SP_ERR_TIMEOUT
+        # the Python path: the watchdog raises on the host once the transform has completed
+        monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
+        xr = torch.from_numpy(rng.standard_normal(2 * n).astype(np.float32)).cuda()
+        bfft.rfft(xr)
+        with pytest.raises(bfft.DeviceWaitTimeout) as info:
+            bfft.device_status()
+        assert info.value.status == _lib.SP_ERR_TIMEOUT
+    finally:
+        lib.sp_fft_set_wait_limit(prev)
+    assert bfft.device_status() == 0  # nothing outstanding
+    # the context stays usable: default limit, clean word, correct result
+    assert lib.sp_fft_c64(x.data_ptr(), out.data_ptr(), 1, n, 0, ws.data_ptr(), ws.numel(),
+                          stream) == 0
+    torch.cuda.synchronize()
+    assert int(ws[off.value : off.value + 4].view(torch.int32).item()) == 0
+    ref = np.fft.fft(x.cpu().numpy().astype(np.complex128))
+    assert _rel(out, ref) < 5e-6
+    xr = torch.from_numpy(rng.standard_normal(2 * n).astype(np.float32)).cuda()
+    got = bfft.rfft(xr)
+    assert bfft.device_status() == 0
+    assert _rel(got, np.fft.rfft(xr.cpu().numpy().astype(np.float64))) < 5e-6
+
+
 def test_default_routing_uses_cufft_below_2p20(rng, monkeypatch):
     monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 20)
     assert not bfft._pow2_in_range(1 << 19) and bfft._pow2_in_range(1 << 20)

@@ -1,6 +1,7 @@
-"""Named, seeded workloads for profiling the kernels from the command line:
+"""Named, seeded workloads for profiling the kernels from the command line (the commands of the
+ncu summaries under profiles/ run these):
 
-    python -m mlx_signal_b200.workloads NAME [NAME ...] [--repeat K]
+    python workloads.py NAME [NAME ...] [--repeat K]
 
 Each workload builds its inputs on the current CUDA device (seeded N(0,1) float32) and runs its
 public call K times (default 1), so a profiler's kernel filter and launch count select exactly
@@ -12,8 +13,12 @@ from __future__ import annotations
 import argparse
 import sys
 
+from pathlib import Path
+
 import numpy as np
 import torch
+
+sys.path.insert(0, str(Path(__file__).resolve().parent))
 
 __all__ = ["WORKLOADS", "run"]
 
@@ -63,7 +68,7 @@ def _istft(msig, k):
 
 
 def _batch48(msig, k):
-    from . import batch
+    from mlx_signal_b200 import batch
 
     rng = np.random.default_rng(3)
     sigs = []
