@@ -37,6 +37,12 @@ struct MeanCfg {
                                  + size_t(TEAMS) * PL::BUF * 8;    // exchange buffers
 };
 
+// k_welch_mean's shared memory: the MeanCfg layout plus one L-float blocked-sum total per team.
+template <class CFG>
+constexpr size_t welch_mean_smem() {
+  return CFG::SMEM + size_t(CFG::TEAMS) * CFG::PL::L * 4;
+}
+
 struct MeanSmem {
   float4* scratch;
   float* win;
@@ -87,6 +93,28 @@ __device__ __forceinline__ void load_pair(float2 (&v)[PL::E], const float* __res
 // 0.5 * P2_k is the sum of |X_s[k]|^2 over both segments of every pair).
 __host__ __device__ constexpr int welch_slot_floats(int L) { return L / 2 + 1; }
 
+// Two-level blocked summation of the welch kernels' per-bin sums: each thread sums the |Z|^2
+// terms of kFoldPairs pairs of segments in registers, then adds that block into a team total in
+// shared memory (tot[e * P + t], FP32). The rounding error of a team's sum then grows with
+// kFoldPairs + pairs / kFoldPairs instead of with the number of pairs; the cross-team sum of the
+// partial slots is FP64 (k_reduce_mean).
+constexpr int kFoldPairs = 8;
+
+template <int E, int P>
+__device__ __forceinline__ void fold_block(float (&acc)[E], float* tot, int t) {
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    tot[e * P + t] += acc[e];
+    acc[e] = 0.f;
+  }
+}
+
+template <int E, int P>
+__device__ __forceinline__ void zero_total(float* tot, int t) {
+#pragma unroll
+  for (int e = 0; e < E; ++e) tot[e * P + t] = 0.f;
+}
+
 // Write a team's per-bin accumulators (bin k = t + e*P in acc[e]) as mirror-combined partials
 // dst[k] = acc_k + acc_{L-k}, k in [0, L/2], staging through the (free) exchange buffer; resets
 // acc.
@@ -121,6 +149,7 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
+  float* tot = reinterpret_cast<float*>(sm.buf + CFG::TEAMS * PL::BUF) + team * L;
   float acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = 0.f;
@@ -130,6 +159,8 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
     const int64_t lim = int64_t(s0) + (gend - g);
     const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
     const float* xr = pr.x + r * pr.ld_x;
+    zero_total<E, P>(tot, t);
+    int npairs = 0;
     for (int s = s0; s < s1; s += 2) {
       const bool two = s + 1 < s1;
       const float* xa = xr + int64_t(s) * pr.hop;
@@ -143,7 +174,13 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
         acc[e] = fmaf(v[e].x, v[e].x, acc[e]);
         acc[e] = fmaf(v[e].y, v[e].y, acc[e]);
       }
+      if (++npairs == kFoldPairs) {
+        npairs = 0;
+        fold_block<E, P>(acc, tot, t);
+      }
     }
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[e] += tot[e * P + t];
     const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
     flush_mirror<PL>(acc, pr.partial + (r * pr.cmax + slot) * int64_t(welch_slot_floats(L)), buf,
                      t, mask);
@@ -210,6 +247,12 @@ struct HalfSmem {
                                   size_t(CFG::TEAMS) * PL::BUF * 8;
 };
 
+// k_welch_half's shared memory: the HalfSmem layout plus one L-float blocked-sum total per team.
+template <class CFG>
+constexpr size_t welch_half_smem() {
+  return HalfSmem<CFG>::BYTES + size_t(CFG::TEAMS) * CFG::PL::L * 4;
+}
+
 // Welch for the 50%-overlap case nperseg == nfft == L, hop == L/2 (the reference's default
 // noverlap = nperseg/2). A pair of segments (s, s+1) spans three half-blocks A | B | C of the row:
 // x_s = A|B, x_{s+1} = B|C, and the next pair's A is this pair's C. Each half-block is loaded once
@@ -226,9 +269,12 @@ struct HalfSmem {
 // last segment runs the same step with the second segment zero. WT: window from the transposed
 // table (HalfWinT) instead of the plain one. SPLIT = false keeps one loop with a runtime
 // lone-segment flag (less code, for kernels that already run near their register limit).
+// tot: optional blocked-sum team total (tot[e * P + t]); when given, acc is folded into it every
+// kFoldPairs pairs (the caller zeroes it and adds it back at the end of the range).
 template <class PL, int DET, bool WT = false, bool SPLIT = true>
 __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const float* __restrict__ xr,
-                                                 int s0, int s1, float (&acc)[PL::E]) {
+                                                 int s0, int s1, float (&acc)[PL::E],
+                                                 float* tot = nullptr) {
   constexpr int L = PL::L, E = PL::E, P = PL::P, H = L / 2, EH = E / 2;
   constexpr int R0 = PL::radix(0), B0 = E / R0;
   static_assert(!WT || HalfWinT<PL>::USE, "transposed window needs E >= 4");
@@ -236,6 +282,7 @@ __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const flo
   const float inv_n = 1.0f / float(L);
   float A[EH], B[EH], C[EH];
   bool carry = false;
+  int npairs = 0;
   float sum_c = 0.f;  // team total of the carried half-block (this pair's A)
   auto step = [&](int s, auto two_c) {
     const bool TWO = bool(two_c);  // a compile-time constant for std::true_type / false_type
@@ -315,6 +362,10 @@ __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const flo
 #pragma unroll
     for (int i = 0; i < EH; ++i) A[i] = C[i];
     carry = true;
+    if (tot != nullptr && ++npairs == kFoldPairs) {
+      npairs = 0;
+      fold_block<E, P>(acc, tot, t);
+    }
   };
   if constexpr (SPLIT) {
     int s = s0;
@@ -375,6 +426,7 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
+  float* tot = reinterpret_cast<float*>(sbuf + CFG::TEAMS * PL::BUF) + team * L;
   float acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = 0.f;
@@ -383,7 +435,10 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
     const int s0 = int(g - r * pr.nseg);
     const int64_t lim = int64_t(s0) + (gend - g);
     const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
-    welch_half_range<PL, DET, WT>(c, pr.x + r * pr.ld_x, s0, s1, acc);
+    zero_total<E, P>(tot, c.t);
+    welch_half_range<PL, DET, WT>(c, pr.x + r * pr.ld_x, s0, s1, acc, tot);
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[e] += tot[e * P + c.t];
     const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
     flush_mirror<PL>(acc, pr.partial + (r * pr.cmax + slot) * int64_t(welch_slot_floats(L)),
                      c.buf, c.t, c.mask);

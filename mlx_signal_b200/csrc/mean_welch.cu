@@ -13,7 +13,7 @@ struct F {
     MeanInfo k;
     k.fn = reinterpret_cast<const void*>(&k_welch_mean<LOG_L, team_log_e<LOG_L>(), DET>);
     k.threads = CFG::THREADS;
-    k.smem = CFG::SMEM;
+    k.smem = welch_mean_smem<CFG>();
     k.teams = CFG::TEAMS;
     k.launch = &launch;
     return k;

@@ -24,6 +24,7 @@ stft (spectral.py:694-738) call.
 from __future__ import annotations
 
 import collections
+import gc
 import time
 from dataclasses import dataclass, field
 
@@ -357,23 +358,44 @@ def poisson_schedule(rate: float, duration: float, pool: torch.Tensor, seed: int
     return sched
 
 
+class _CollectorPaused:
+    """Pause Python's cyclic garbage collector for a request loop. A full collection walks every
+    tracked object (request tuples, tensor views, per-request records): with tens of thousands
+    of requests queued it stalls the loop for tens to hundreds of milliseconds, which shows up
+    as p99 latency. Reference counting still frees everything; the collector is re-enabled (and
+    run once) when the loop ends."""
+
+    def __enter__(self):
+        self.was = gc.isenabled()
+        gc.collect()
+        gc.disable()
+        return self
+
+    def __exit__(self, *exc):
+        if self.was:
+            gc.enable()
+        return False
+
+
 def run_schedule(server: SpectralServer, schedule) -> ServerStats:
     """Drive `server` with an open-loop arrival schedule (arrival times relative to the start):
     each request is submitted when its time comes, and the loop keeps stepping until all have
-    completed. Latencies count from the scheduled arrival."""
-    t0 = time.perf_counter()
-    i = 0
-    n = len(schedule)
-    while i < n or server.pending or server.inflight:
-        now = time.perf_counter()
-        while i < n and t0 + schedule[i][0] <= now:
-            arr, kind, x, p = schedule[i]
-            if kind == KIND_WELCH:
-                server.submit_welch(x, nperseg=p["nperseg"], arrival=t0 + arr)
-            else:
-                server.submit_chunk(p["stream"], x, arrival=t0 + arr)
-            i += 1
-        server.step()
+    completed. Latencies count from the scheduled arrival. The loop runs with the cyclic
+    garbage collector paused (_CollectorPaused)."""
+    with _CollectorPaused():
+        t0 = time.perf_counter()
+        i = 0
+        n = len(schedule)
+        while i < n or server.pending or server.inflight:
+            now = time.perf_counter()
+            while i < n and t0 + schedule[i][0] <= now:
+                arr, kind, x, p = schedule[i]
+                if kind == KIND_WELCH:
+                    server.submit_welch(x, nperseg=p["nperseg"], arrival=t0 + arr)
+                else:
+                    server.submit_chunk(p["stream"], x, arrival=t0 + arr)
+                i += 1
+            server.step()
     return server.stats
 
 
@@ -381,7 +403,13 @@ def run_per_request(schedule, fs: float = 1.0, window="hann", stream_nperseg: in
                     stream_noverlap: int = 768, max_streams: int = 256):
     """The plain per-request path on an arrival schedule: (arrival, kind, payload, params) in
     arrival order, processed FIFO on the current stream as soon as each arrives; completion is
-    observed through one CUDA event per request. Returns ServerStats."""
+    observed through one CUDA event per request. Runs with the garbage collector paused, as
+    run_schedule does. Returns ServerStats."""
+    with _CollectorPaused():
+        return _run_per_request(schedule, fs, window, stream_nperseg, stream_noverlap)
+
+
+def _run_per_request(schedule, fs, window, stream_nperseg, stream_noverlap):
     from .spectral import stft, welch
 
     stats = ServerStats()

@@ -46,6 +46,12 @@ def rfft(x):
     return np.fft.rfft(x)
 
 
+def welch_f64(x, **kw):
+    """The float64 oracle: scipy.signal.welch on the input upcast to float64 (the reference's
+    tests compute their goldens this way, tests/test_spectral.py:38-47)."""
+    return sps.welch(np.asarray(x, dtype=np.float64), **kw)
+
+
 def _rows_task(fn_name: str, kw: dict, arrays: tuple[np.ndarray, ...]):
     fn = globals()[fn_name]
     return fn(*arrays, **kw)
