@@ -23,6 +23,9 @@ constexpr int kRedGroups = 8;
 
 __global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p) {
   pdl_wait();  // launched as a programmatic dependent of the segment kernel
+  // the next kernel in the stream (e.g. the next call's segment kernel, which waits for this
+  // grid to complete before reading anything the caller passes) may start its prologue now
+  pdl_trigger();
   __shared__ double4 red[kRedGroups][32];
   const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
   const int64_t chunks = (p.nout + 31) / 32;

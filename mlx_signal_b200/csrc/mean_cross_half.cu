@@ -11,7 +11,7 @@ struct Mode {
     static constexpr int LL = LOG_L < 1 ? 1 : LOG_L;
     static constexpr int DD = DET == 2 ? kDetrendConstantSpectral : DET;
     static void launch(dim3 g, int t, size_t sm, cudaStream_t st, const MeanParams& p) {
-      k_cross_half<LL, team_log_e<LL>(), DD, CSD><<<g, t, sm, st>>>(p);
+      launch_half(k_cross_half<LL, team_log_e<LL>(), DD, CSD>, g, t, sm, st, p);
     }
     static MeanInfo get() {
       using CFG = MeanCfg<LL, team_log_e<LL>()>;

@@ -1,8 +1,6 @@
 // Instantiations of k_welch_half (50%-overlap welch) for every fused nfft >= 2; lookup detrend
-// index 0 none, 1 constant (time domain), 2 constant (spectral correction). nfft 1024 runs the
-// packed-f32x2 kernel (welch_packed.cuh).
+// index 0 none, 1 constant (time domain), 2 constant (spectral correction).
 #include "dispatch.cuh"
-#include "welch_packed.cuh"
 
 namespace b2s {
 namespace {
@@ -11,25 +9,15 @@ struct F {
   static constexpr int LL = LOG_L < 1 ? 1 : LOG_L;
   // lookup index 2 selects the spectral constant detrend
   static constexpr int DD = DET == 2 ? kDetrendConstantSpectral : DET;
-  static constexpr bool PACKED = LL == 10;
   static void launch(dim3 g, int t, size_t sm, cudaStream_t st, const MeanParams& p) {
-    if constexpr (PACKED) {
-      k_welch_half_packed<DD><<<g, t, sm, st>>>(p);
-    } else {
-      k_welch_half<LL, team_log_e<LL>(), DD><<<g, t, sm, st>>>(p);
-    }
+    launch_half(k_welch_half<LL, team_log_e<LL>(), DD>, g, t, sm, st, p);
   }
   static MeanInfo get() {
     using CFG = MeanCfg<LL, team_log_e<LL>()>;
     MeanInfo k;
-    if constexpr (PACKED) {
-      k.fn = reinterpret_cast<const void*>(&k_welch_half_packed<DD>);
-      k.smem = pk::Smem<CFG>::BYTES;
-    } else {
-      k.fn = reinterpret_cast<const void*>(&k_welch_half<LL, team_log_e<LL>(), DD>);
-      k.smem = welch_half_smem<CFG>();
-    }
+    k.fn = reinterpret_cast<const void*>(&k_welch_half<LL, team_log_e<LL>(), DD>);
     k.threads = CFG::THREADS;
+    k.smem = welch_half_smem<CFG>();
     k.teams = CFG::TEAMS;
     k.launch = &launch;
     return k;

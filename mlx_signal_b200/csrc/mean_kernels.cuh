@@ -195,6 +195,25 @@ __device__ __forceinline__ void pdl_trigger() {
 }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Launch a 50%-overlap kernel as a programmatic dependent of the stream's previous kernel: its
+// CTAs become resident and build their constant tables while that kernel (typically the previous
+// call's reduction) finishes; they read the caller's buffers only after griddepcontrol.wait.
+template <class K>
+inline void launch_half(K kernel, dim3 g, int threads, size_t smem, cudaStream_t s,
+                        const MeanParams& p) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = dim3(unsigned(threads));
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  (void)cudaLaunchKernelEx(&cfg, kernel, p);  // errors surface through cudaGetLastError
+}
+
 // Shared-memory tables and team coordinates used by the half-overlap pair loop.
 template <class PL>
 struct HalfCtx {
@@ -401,6 +420,11 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   float2* whi = wlo + P;                                              // DFT(win)_{L-P+t}
   float2* tw = whi + P;
   float2* sbuf = tw + PL::TW;
+  // the twiddles come from a constant table; everything the caller passes (window, window
+  // spectrum, signal) is read only after the stream's previous kernel has completed: the kernel
+  // may be launched as a programmatic dependent of it (launch_half)
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  pdl_wait();
   if constexpr (WT) {
     build_half_wint<PL>(win1, pr.win, threadIdx.x);
   } else {
@@ -408,7 +432,6 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   }
   if constexpr (DET == kDetrendConstantSpectral)
     load_window_lowbins<P>(wlo, whi, pr.wdft, pr.n_low, threadIdx.x, blockDim.x);
-  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
   __syncthreads();
   pdl_trigger();
   const int team = threadIdx.x / P;
@@ -550,6 +573,11 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   float2* whi = wlo + P;
   float2* tw = whi + P;
   float2* sbuf = tw + PL::TW;
+  // the twiddles come from a constant table; everything the caller passes (window, window
+  // spectrum, signal) is read only after the stream's previous kernel has completed: the kernel
+  // may be launched as a programmatic dependent of it (launch_half)
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  pdl_wait();
   if constexpr (WT) {
     build_half_wint<PL>(win1, pr.win, threadIdx.x);
   } else {
@@ -557,7 +585,6 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   }
   if constexpr (DET == kDetrendConstantSpectral)
     load_window_lowbins<P>(wlo, whi, pr.wdft, pr.n_low, threadIdx.x, blockDim.x);
-  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
   __syncthreads();
   pdl_trigger();
   const int team = threadIdx.x / P, t = threadIdx.x - team * P;
