@@ -593,6 +593,7 @@ def secondary(x, steps, warmup, dist, clocks):
     out["general_shapes"] = general_shapes(x, dist, clocks, peak)
     out["batched_512_uneven"] = batched_uneven(dist, clocks, peak)
     out["rfft_1x2p23"] = large_rfft(dist, clocks, peak)
+    out["tc_dft32_stage"] = tc_dft32_stage(dist, clocks)
     out["fft_consumers"] = fft_consumers(dist, clocks, peak)
     out["reference_published_rows"] = published_rows(dist, clocks)
     return out
@@ -850,6 +851,40 @@ def batched_uneven(dist, clocks, peak, nreq=512, seed=11):
     return res
 
 
+def tc_dft32_stage(dist, clocks, seed=17):
+    """The radix-32 DFT stage on the tensor cores (sp_dft32_tc_c64: FP16 head/tail splits, three
+    products, FP32 accumulation) on the vector count of one radix-32 pass of the 64 x 2^20 welch
+    (65,504 pair transforms x 32 columns): its tensor-core rate with the operands staged (the MMA
+    chain repeated 16 times) and end to end, its error against float64 numpy, and what one pass
+    costs at that rate beside the whole CUDA-core welch."""
+    import torch
+
+    from mlx_signal_b200 import _kernels
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    nvec = 65504 * 32
+    z = torch.complex(torch.randn(nvec, 32, generator=g, device=dev),
+                      torch.randn(nvec, 32, generator=g, device=dev))
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    res = {"vectors": nvec, "mma": "tcgen05 kind::f16 M128 N64 K192 (3 split products)"}
+    for reps in (1, 16):
+        ms = timed(lambda: _kernels.dft32_tc(z, reps=reps, err=err), 10, 3, dist, clocks)
+        res[f"reps{reps}_ms"] = ms
+        res[f"reps{reps}_tc_tflops_issued"] = nvec * 2 * 64 * 192 * reps / ms / 1e9
+    res["tc_time_per_pass_ms"] = res["reps16_ms"] / 16
+    res["error_word"] = int(err.item())
+    if dist is None:
+        y = _kernels.dft32_tc(z[:8192])
+        ref = np.fft.fft(z[:8192].cpu().numpy().astype(np.complex128), axis=-1)
+        e = np.abs(y.cpu().numpy() - ref).max(axis=-1) / np.abs(ref).max(axis=-1)
+        res["max_err_rel_peak_vs_numpy_f64"] = float(e.max())
+        res["median_err_rel_peak_vs_numpy_f64"] = float(np.median(e))
+    del z
+    return res
+
+
 def large_rfft(dist, clocks, peak, log_n=23, seed=5):
     """1 x 2^23 float32 N(0,1) real FFT through the three-pass path, against numpy float64."""
     import torch
@@ -924,6 +959,11 @@ def summarize(sec: dict) -> dict:
     if "rfft_1x2p23" in sec:
         ms["rfft_2p23"] = [r(sec["rfft_1x2p23"]["ms"] * 1e3), r(sec["rfft_1x2p23"]["frac_hbm"])]
     out["us_and_frac_hbm"] = ms
+    if "tc_dft32_stage" in sec:
+        tc = sec["tc_dft32_stage"]
+        out["tc_dft32_pass"] = {"us": r(tc["tc_time_per_pass_ms"] * 1e3),
+                                "tflops": r(tc["reps16_tc_tflops_issued"]),
+                                "err": r(tc.get("max_err_rel_peak_vs_numpy_f64"))}
     return out
 
 

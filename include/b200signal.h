@@ -298,6 +298,20 @@ SP_API int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_
 SP_API uint32_t sp_fft_set_wait_limit(uint32_t polls);
 
 /*
+ * Batched 32-point complex DFTs on the tensor cores: y[v] = DFT_32(z[v]) for v < nvec (z, y:
+ * nvec x 32 interleaved complex64, 16-byte aligned device pointers). Each tile of 128 vectors is
+ * one tcgen05 GEMM (M 128, N 64, K 192) over FP16 head/tail splits of the vectors and of the
+ * DFT matrix (three products, FP32 accumulation in tensor memory; each vector scaled by a power
+ * of two into the FP16 range first): error ~1e-7 of the vector's peak, the class of an FP32 FFT.
+ * reps > 1 repeats the MMA chain on the staged operands (same result) to measure the tensor-core
+ * rate alone. err_word (device int, may be NULL) receives SP_ERR_TIMEOUT if the bounded wait for
+ * the MMAs runs out. The radix-32 DFT stage of the framed FFTs, which the reference computes as
+ * radix-2 threadgroup butterflies (_stft_metal.py:124-144), on the tensor cores.
+ */
+SP_API int sp_dft32_tc_c64(const float* z, float* y, int64_t nvec, int reps, int* err_word,
+                           void* stream);
+
+/*
  * FFT convolution of each of `rows` real rows x (n1 samples, row stride ld_x) with one real filter
  * h of n2 <= 2049 taps: out[r * ld_out + i] = (x_r * h)[j0 + i] for i in [0, nout), where
  * (x_r * h)[j] = sum_k h[k] x_r[j - k] is the full linear convolution (length n1 + n2 - 1;

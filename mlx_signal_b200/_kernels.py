@@ -350,3 +350,20 @@ def csd_complex(x: torch.Tensor, y: torch.Tensor, win: torch.Tensor, nperseg: in
                                nperseg, nfft, hop, detrend, out.data_ptr(), ws.data_ptr(),
                                ws.numel(), stream_handle()), "sp_csd_cplx")
     return out
+
+
+def dft32_tc(z: torch.Tensor, reps: int = 1, err: torch.Tensor | None = None) -> torch.Tensor:
+    """32-point complex DFTs of the last axis of z (complex64 CUDA, last dimension 32) on the
+    tensor cores (sp_dft32_tc_c64: FP16 head/tail splits, three products, FP32 accumulation).
+    `reps` repeats the MMA chain on the staged operands (rate measurement; same result). `err`:
+    optional int32 CUDA tensor of one element that receives SP_ERR_TIMEOUT if the bounded wait
+    for the MMAs runs out."""
+    if z.dtype != torch.complex64 or not z.is_cuda or z.shape[-1] != 32:
+        raise ValueError("dft32_tc: complex64 CUDA tensor with a last dimension of 32")
+    zc = z.reshape(-1, 32).contiguous()
+    out = torch.empty_like(zc)
+    lib = _lib.load()
+    _lib.check(lib.sp_dft32_tc_c64(zc.data_ptr(), out.data_ptr(), zc.shape[0], int(reps),
+                                   None if err is None else err.data_ptr(), stream_handle()),
+               "sp_dft32_tc_c64")
+    return out.reshape(z.shape)
