@@ -254,6 +254,28 @@ SP_API int sp_istft_f32(const float* z, int64_t rows, int nseg, int64_t ld_row, 
                         int nbins_in, const float* win, float scale, int nperseg, int hop,
                         float* out, void* stream);
 
+/*
+ * sp_istft_f32 with an FFT length nfft >= nperseg (a power of two in [2, 4096]; any nperseg >= 1):
+ * each frame is the first nperseg samples of the nfft-point inverse real FFT of its one-sided
+ * spectrum (nbins_in <= nfft/2 + 1 bins), windowed by the nperseg-point win; outlen = nperseg +
+ * (nseg-1)*hop. nfft == nperseg is sp_istft_f32. Replaces the composed zero-padded branch of
+ * spectral.istft (spectral.py:929-950: irfft(n=nfft)[:nperseg], then overlap-add).
+ */
+SP_API int sp_istft_f32_ex(const float* z, int64_t rows, int nseg, int64_t ld_row, int ldf,
+                           int nbins_in, const float* win, float scale, int nperseg, int nfft,
+                           int hop, float* out, void* stream);
+
+/*
+ * Two-sided inverse STFT (input_onesided=False): z (rows, nseg, ldf) complex64 two-sided spectra
+ * (bins k < nbins_in <= nfft used, the rest zero); each frame is the first nperseg samples of the
+ * nfft-point inverse complex FFT, windowed, overlap-added and divided by the window energy as in
+ * sp_istft_f32; out (rows, outlen) complex64. nfft a power of two in [2, 4096]. Replaces the
+ * two-sided branch of spectral.istft (spectral.py:929-950: ifft, then overlap-add).
+ */
+SP_API int sp_istft_c64(const float* z, int64_t rows, int nseg, int64_t ld_row, int ldf,
+                        int nbins_in, const float* win, float scale, int nperseg, int nfft,
+                        int hop, float* out, void* stream);
+
 /* Workspace bytes for the long transforms below (two N-point complex intermediates + the device
  * error word; N = n for sp_fft_c64, n/2 for the real transforms). Negative = error status. */
 SP_API int64_t sp_fft_workspace_size(int64_t n, int batch);

@@ -217,23 +217,36 @@ def frames(kind: str, x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: in
     raise ValueError(kind)
 
 
-def istft_fused(z: torch.Tensor, win: torch.Tensor, scale: float, nperseg: int, hop: int
-                ) -> torch.Tensor:
-    """Fused inverse STFT of (rows, nseg, nf) complex64 one-sided spectra (bins contiguous):
-    irfft per frame, window * scale, overlap-add and division by the window energy (where it
-    exceeds 1e-10) in one kernel -> (rows, nperseg + (nseg-1)*hop) float32."""
+def istft_fused(z: torch.Tensor, win: torch.Tensor, scale: float, nperseg: int, hop: int,
+                nfft: int | None = None, onesided: bool = True) -> torch.Tensor:
+    """Fused inverse STFT of (rows, nseg, nf) complex64 spectra (bins contiguous): inverse FFT of
+    length nfft (default nperseg) per frame -- irfft of one-sided spectra, ifft of two-sided
+    ones -- its first nperseg samples times win * scale, overlap-add and division by the window
+    energy (where it exceeds 1e-10) in one kernel -> (rows, nperseg + (nseg-1)*hop) float32, or
+    complex64 for two-sided input."""
     assert z.is_cuda and z.dtype == torch.complex64 and z.dim() == 3
     if z.stride(2) != 1 or z.stride(1) < z.shape[2] or z.stride(0) < z.shape[1] * z.stride(1):
         z = z.contiguous()
+    nfft = nperseg if nfft is None else int(nfft)
     rows, nseg, nf = z.shape
     outlen = nperseg + (nseg - 1) * hop
-    out = torch.empty((rows, outlen), dtype=torch.float32, device=z.device)
     ld_row = z.stride(0) if rows > 1 else nseg * z.stride(1)
+    lib = _lib.load()
+    if onesided:
+        out = torch.empty((rows, outlen), dtype=torch.float32, device=z.device)
+        _lib.check(
+            lib.sp_istft_f32_ex(z.data_ptr(), rows, nseg, ld_row, z.stride(1), nf,
+                                win.data_ptr(), float(scale), nperseg, nfft, hop, out.data_ptr(),
+                                stream_handle()),
+            "sp_istft_f32_ex",
+        )
+        return out
+    out = torch.empty((rows, outlen), dtype=torch.complex64, device=z.device)
     _lib.check(
-        _lib.load().sp_istft_f32(z.data_ptr(), rows, nseg, ld_row, z.stride(1), nf,
-                                 win.data_ptr(), float(scale), nperseg, hop, out.data_ptr(),
-                                 stream_handle()),
-        "sp_istft_f32",
+        lib.sp_istft_c64(z.data_ptr(), rows, nseg, ld_row, z.stride(1), min(nf, nfft),
+                         win.data_ptr(), float(scale), nperseg, nfft, hop, out.data_ptr(),
+                         stream_handle()),
+        "sp_istft_c64",
     )
     return out
 

@@ -95,6 +95,14 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         c_i,
         [c_fp, c_i64, c_i, c_i64, c_i, c_i, c_fp, ctypes.c_float, c_i, c_i, c_fp, c_p],
     ),
+    "sp_istft_f32_ex": (
+        c_i,
+        [c_fp, c_i64, c_i, c_i64, c_i, c_i, c_fp, ctypes.c_float, c_i, c_i, c_i, c_fp, c_p],
+    ),
+    "sp_istft_c64": (
+        c_i,
+        [c_fp, c_i64, c_i, c_i64, c_i, c_i, c_fp, ctypes.c_float, c_i, c_i, c_i, c_fp, c_p],
+    ),
     "sp_fft_workspace_size": (c_i64, [c_i64, c_i]),
     "sp_fft_c64": (c_i, [c_fp, c_fp, c_i, c_i64, c_i, c_p, c_sz, c_p]),
     "sp_rfft_c64": (c_i, [c_fp, c_fp, c_i, c_i64, c_i64, c_p, c_sz, c_p]),

@@ -54,6 +54,7 @@ using FrameInfo = KernelInfo<FrameParams>;
 using IstftInfo = KernelInfo<IstftParams>;
 IstftInfo istft_lookup(int log_l);       // log_l in [1, kMaxLogL]
 IstftInfo istft_half_lookup(int log_l);  // hop == nperseg / 2
+IstftInfo istft_cplx_lookup(int log_l);  // two-sided input, complex output
 
 // family: 0 welch mean, 1 cross mean
 MeanInfo mean_lookup_welch(int log_l, int det);

@@ -30,9 +30,10 @@ struct IstftParams {
   int64_t rows;
   int nseg;
   int hop;
-  const float* win;  // L window values
+  const float* win;  // nper window values
   float scale;       // istft scale (spectrum: sum(win); psd: sqrt(fs sum(win^2)))
-  int64_t outlen;    // L + (nseg - 1) * hop
+  int nper;          // frame length (nperseg <= L): the first nper samples of each inverse FFT
+  int64_t outlen;    // nper + (nseg - 1) * hop
   float* out;        // (rows, outlen)
   int64_t G;         // output frames owned per team
   int64_t total;     // rows * nseg
@@ -64,11 +65,12 @@ __global__ void __launch_bounds__(IstftCfg<LOG_L, LOG_E>::THREADS) k_istft(Istft
   float2* sbuf = tw + PL::TW;
   float* rings = reinterpret_cast<float*>(sbuf + CFG::TEAMS * PL::BUF);
   const int hop = pr.hop;
+  const int N = pr.nper;  // frame length; samples N .. L-1 of each inverse FFT are dropped
   const float fs = pr.scale / float(L);
-  for (int i = threadIdx.x; i < L; i += blockDim.x) weff[i] = pr.win[i] * fs;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) weff[i] = i < N ? pr.win[i] * fs : 0.f;
   for (int r = threadIdx.x; r < hop; r += blockDim.x) {
     float s = 0.f;
-    for (int n = r; n < L; n += hop) s = fmaf(pr.win[n], pr.win[n], s);
+    for (int n = r; n < N; n += hop) s = fmaf(pr.win[n], pr.win[n], s);
     normp[r] = s;
   }
   build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
@@ -82,7 +84,7 @@ __global__ void __launch_bounds__(IstftCfg<LOG_L, LOG_E>::THREADS) k_istft(Istft
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
-  const int halo = (L + hop - 1) / hop - 1;  // frames starting left of a range that reach into it
+  const int halo = (N + hop - 1) / hop - 1;  // frames starting left of a range that reach into it
   while (g < gend) {
     const int64_t r = g / pr.nseg;
     const int f0 = int(g - r * pr.nseg);
@@ -150,11 +152,11 @@ __global__ void __launch_bounds__(IstftCfg<LOG_L, LOG_E>::THREADS) k_istft(Istft
         const int slot = int(o & (RING - 1));
         if (o >= own_lo) {
           float nrm;
-          if (o >= L - hop && o < int64_t(pr.nseg) * hop) {
+          if (o >= N - hop && o < int64_t(pr.nseg) * hop) {
             nrm = normp[res];
           } else {
             nrm = 0.f;
-            int64_t slo = o - L + 1 > 0 ? (o - L + 1 + hop - 1) / hop : 0;
+            int64_t slo = o - N + 1 > 0 ? (o - N + 1 + hop - 1) / hop : 0;
             int64_t shi = o / hop;
             if (shi > pr.nseg - 1) shi = pr.nseg - 1;
             for (int64_t q = slo; q <= shi; ++q) {
@@ -174,6 +176,127 @@ __global__ void __launch_bounds__(IstftCfg<LOG_L, LOG_E>::THREADS) k_istft(Istft
     }
     // partial sums past own_hi belong to the next team's range: clear the ring for the next range
     for (int i = t; i < RING; i += P) ring[i] = 0.f;
+    team_sync<P>(mask);
+    g += f1 - f0;
+  }
+}
+
+// Two-sided inverse STFT (input_onesided=False): each frame is its own complex inverse FFT of
+// length L, x_s = IFFT_L(Z_s)[0 : nper] (complex), windowed and overlap-added into a complex
+// shared-memory ring with the window-energy normalisation of k_istft; the output is complex64
+// (scipy's istft returns the complex result for two-sided input). Inverse by conjugation:
+// IFFT(Z) = conj(FFT(conj Z)) / L, the 1/L folded into the window table.
+template <int LOG_L, int LOG_E>
+struct IstftCplxCfg {
+  using PL = Plan<LOG_L, LOG_E>;
+  static constexpr int TEAMS = PL::P >= 64 ? 1 : 128 / PL::P;
+  static constexpr int THREADS = TEAMS * PL::P;
+  static constexpr int SCRATCH = PL::P >= 64 ? PL::P / 32 : 1;
+  static constexpr int WIN = (PL::L + 3) & ~3;
+  static constexpr int RING = 2 * PL::L;  // complex samples: [s*hop, s*hop + nper) for hop <= L
+  static constexpr size_t SMEM = size_t(TEAMS) * SCRATCH * 16 + size_t(WIN) * 4 * 2 +
+                                 size_t(PL::TW) * 8 + size_t(TEAMS) * PL::BUF * 8 +
+                                 size_t(TEAMS) * RING * 8;
+};
+
+template <int LOG_L, int LOG_E>
+__global__ void __launch_bounds__(IstftCplxCfg<LOG_L, LOG_E>::THREADS)
+    k_istft_cplx(IstftParams pr) {
+  using CFG = IstftCplxCfg<LOG_L, LOG_E>;
+  using PL = typename CFG::PL;
+  constexpr int L = PL::L, E = PL::E, P = PL::P, RING = CFG::RING;
+  extern __shared__ float4 smem[];
+  float* weff = reinterpret_cast<float*>(smem + CFG::TEAMS * CFG::SCRATCH);  // win*scale/L
+  float* normp = weff + CFG::WIN;  // periodic window-energy table, index o mod hop
+  float2* tw = reinterpret_cast<float2*>(normp + CFG::WIN);
+  float2* sbuf = tw + PL::TW;
+  float2* rings = sbuf + CFG::TEAMS * PL::BUF;
+  const int hop = pr.hop;
+  const int N = pr.nper;
+  const float fs = pr.scale / float(L);
+  for (int i = threadIdx.x; i < L; i += blockDim.x) weff[i] = i < N ? pr.win[i] * fs : 0.f;
+  for (int r = threadIdx.x; r < hop; r += blockDim.x) {
+    float s = 0.f;
+    for (int n = r; n < N; n += hop) s = fmaf(pr.win[n], pr.win[n], s);
+    normp[r] = s;
+  }
+  build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int team = threadIdx.x / P, t = threadIdx.x - team * P;
+  const unsigned mask = team_mask<P>();
+  float2* buf = sbuf + team * PL::BUF;
+  float2* ring = rings + team * RING;
+  for (int i = t; i < RING; i += P) ring[i] = make_float2(0.f, 0.f);
+  team_sync<P>(mask);
+  const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
+  int64_t g = tau * pr.G;
+  const int64_t gend = min(g + pr.G, pr.total);
+  const int halo = (N + hop - 1) / hop - 1;
+  float2* out = reinterpret_cast<float2*>(pr.out);
+  while (g < gend) {
+    const int64_t r = g / pr.nseg;
+    const int f0 = int(g - r * pr.nseg);
+    const int64_t lim = int64_t(f0) + (gend - g);
+    const int f1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
+    const int64_t own_lo = int64_t(f0) * hop;
+    const int64_t own_hi = f1 == pr.nseg ? pr.outlen : int64_t(f1) * hop;
+    const int sa = f0 - halo > 0 ? f0 - halo : 0;
+    const float2* zr = pr.z + r * pr.ld_row;
+    float2* orow = out + r * pr.outlen;
+    int64_t done = int64_t(sa) * hop;
+    for (int s = sa; s < f1; ++s) {
+      const float2* za = zr + int64_t(s) * pr.ldf;
+      float2 v[E];
+      static_for<0, E>([&](auto ec) {
+        constexpr int e = decltype(ec)::value;
+        const int k = slot_elem<PL, e>(t);
+        const float2 a = k < pr.nbins_in ? za[k] : make_float2(0.f, 0.f);
+        v[e] = make_float2(a.x, -a.y);  // conj
+      });
+      team_pass0<PL>(v);
+      team_passes<PL>(v, buf, tw, t, mask);
+      // x_s[n] = conj(v[n]) / L, the 1/L in weff
+      const int64_t pa = int64_t(s) * hop;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int n = t + e * P;
+        float2& q = ring[(pa + n) & (RING - 1)];
+        q.x = fmaf(v[e].x, weff[n], q.x);
+        q.y = fmaf(-v[e].y, weff[n], q.y);
+      }
+      team_sync<P>(mask);
+      const bool last = s + 1 >= f1;
+      const int64_t fin = last ? own_hi : int64_t(s + 1) * hop;
+      int res = int((done + t) % hop);
+      const int pstep = P % hop;
+      for (int64_t o = done + t; o < fin; o += P) {
+        const int slot = int(o & (RING - 1));
+        if (o >= own_lo) {
+          float nrm;
+          if (o >= N - hop && o < int64_t(pr.nseg) * hop) {
+            nrm = normp[res];
+          } else {
+            nrm = 0.f;
+            int64_t slo = o - N + 1 > 0 ? (o - N + 1 + hop - 1) / hop : 0;
+            int64_t shi = o / hop;
+            if (shi > pr.nseg - 1) shi = pr.nseg - 1;
+            for (int64_t q = slo; q <= shi; ++q) {
+              const float w = pr.win[o - q * hop];
+              nrm = fmaf(w, w, nrm);
+            }
+          }
+          const float2 val = ring[slot];
+          const float d = nrm > 1e-10f ? nrm : 1.0f;
+          orow[o] = make_float2(val.x / d, val.y / d);
+        }
+        ring[slot] = make_float2(0.f, 0.f);
+        res += pstep;
+        if (res >= hop) res -= hop;
+      }
+      done = fin;
+      team_sync<P>(mask);
+    }
+    for (int i = t; i < RING; i += P) ring[i] = make_float2(0.f, 0.f);
     team_sync<P>(mask);
     g += f1 - f0;
   }

@@ -781,8 +781,10 @@ class _IstftPlan:
     the NOLA verdict and the output time vector, derived once."""
 
     def __init__(self, win, scale, nperseg, nstep, batch, outputlength, boundary, nola_ok, perm,
-                 fs, freq_ax, time_ax):
+                 fs, freq_ax, time_ax, nfft=None, onesided=True):
         self.win, self.scale, self.nperseg, self.nstep = win, scale, nperseg, nstep
+        self.nfft = nperseg if nfft is None else nfft
+        self.onesided = onesided
         self.batch, self.outputlength, self.boundary = batch, outputlength, boundary
         self.nola_ok, self.perm, self.fs = nola_ok, perm, fs
         self.freq_ax, self.time_ax = freq_ax, time_ax
@@ -792,7 +794,7 @@ class _IstftPlan:
         if not permuted and self.perm != list(range(Z.dim())):
             Z = Z.permute(self.perm)
         x = _kernels.istft_fused(Z.reshape((self.rows,) + Z.shape[-2:]), self.win, self.scale,
-                                 self.nperseg, self.nstep)
+                                 self.nperseg, self.nstep, self.nfft, self.onesided)
         x = x.reshape(self.batch + (self.outputlength,))
         if self.boundary:
             x = x[..., self.nperseg // 2 : -(self.nperseg // 2)]
@@ -876,18 +878,19 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
         raise ValueError(f"Parameter {scaling=} not in ['spectrum', 'psd']!")
     outputlength = nperseg + (nseg - 1) * nstep
     batch = Z.shape[:-2]
-    if input_onesided and nfft == nperseg and _kernels.is_pow2(nperseg) and \
-            2 <= nperseg <= _kernels.MAX_FUSED_NFFT:
+    if _kernels.is_pow2(nfft) and 2 <= nfft <= _kernels.MAX_FUSED_NFFT:
+        # fused: one-sided (irfft) or two-sided (ifft, complex output) spectra, frames of
+        # nperseg <= nfft samples
         plan = _IstftPlan(device_vector(win_np.astype(np.float32)), scale, nperseg, nstep,
                           batch, outputlength, bool(boundary),
                           _nola_ok(win_np, nperseg, nstep, nseg, outputlength, bool(boundary)),
-                          perm, fs, freq_ax, time_ax)
+                          perm, fs, freq_ax, time_ax, nfft, bool(input_onesided))
         if key is not None:
             if len(_ISTFT_PLANS) >= 256:
                 _ISTFT_PLANS.clear()
             _ISTFT_PLANS[key] = plan
         return plan.run(Z, permuted=True)
-    composed_path_notice("istft", "composed inverse path")
+    composed_path_notice("istft", "non-power-of-two nfft (composed inverse path)")
     if input_onesided:
         xsubs = torch.fft.irfft(Z, n=nfft, dim=-1)[..., :nperseg]
     else:

@@ -498,3 +498,42 @@ def test_complex_input_spectrogram_matches_scipy(rng, mode):
     f, t, s = msig.spectrogram(x, **kw)
     assert tuple(s.shape) == s_ref.shape
     assert_close(s, s_ref)
+
+
+@pytest.mark.parametrize("nperseg,nfft,noverlap", [(200, 256, 100), (256, 512, 128),
+                                                  (256, 512, 200), (100, 128, 25),
+                                                  (1000, 1024, 500)])
+def test_istft_zero_padded_fused(rng, nperseg, nfft, noverlap):
+    """nfft > nperseg (any nperseg): the fused kernel inverts nfft-point spectra and keeps the
+    first nperseg samples of each frame; no composed-path warning."""
+    import warnings
+
+    x = make_sig(rng, (2, 6000))
+    kw = dict(nperseg=nperseg, nfft=nfft, noverlap=noverlap)
+    _, _, z = sps.stft(x.astype(np.float64), **kw)
+    t_ref, x_ref = sps.istft(z, **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", msig.FallbackWarning)
+        warnings.simplefilter("ignore", msig.DowncastWarning)
+        t2, x2 = msig.istft(z, **kw)
+    assert x_ref.shape == tuple(x2.shape)
+    assert len(t2) == x_ref.shape[-1]  # (scipy's t of an N-d input has the first axis' length)
+    assert_close(x2, x_ref)
+
+
+@pytest.mark.parametrize("kw", [{}, {"nperseg": 128, "noverlap": 96}, {"nperseg": 200,
+                                                                       "nfft": 256}])
+def test_istft_two_sided_complex_fused(rng, kw):
+    """Two-sided spectra of a complex signal: fused complex inverse + overlap-add, complex64
+    output equal to scipy's."""
+    import warnings
+
+    x = (make_sig(rng, (3000,)) + 1j * make_sig(rng, (3000,))).astype(np.complex128)
+    _, _, z = sps.stft(x, return_onesided=False, **kw)
+    _, x_ref = sps.istft(z, input_onesided=False, **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", msig.FallbackWarning)
+        warnings.simplefilter("ignore", msig.DowncastWarning)
+        _, x2 = msig.istft(z, input_onesided=False, **kw)
+    assert x2.is_complex() and x_ref.shape == tuple(x2.shape)
+    assert_close(x2, x_ref)
