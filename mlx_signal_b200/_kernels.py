@@ -24,7 +24,18 @@ def is_pow2(v: int) -> bool:
     return v >= 1 and (v & (v - 1)) == 0
 
 
+#: longest power-of-two nfft of the real-input segment-mean and per-frame kernels
+MAX_FUSED_NFFT_REAL = 8192
+
+
 def fused_mean_ok(nfft: int) -> bool:
+    """A power-of-two nfft the real-input kernels (welch, csd, coherence, stft, spectrogram)
+    compute fused."""
+    return is_pow2(nfft) and nfft <= MAX_FUSED_NFFT_REAL
+
+
+def fused_complex_ok(nfft: int) -> bool:
+    """A power-of-two nfft the complex-input kernels compute fused."""
     return is_pow2(nfft) and nfft <= MAX_FUSED_NFFT
 
 

@@ -37,9 +37,9 @@ int run_frames(int kind, const float* x, const float* y, int64_t rows, int64_t n
   const int log_l = ilog2_exact(nfft);
   // stft / spectrogram with a non-power-of-two nfft: the Bluestein frame kernels
   const bool blue = log_l < 0 && kind != kFrameCross && nfft >= 3 && nfft <= kBlueMaxN;
-  if (!blue && (log_l < 0 || log_l > kMaxLogL)) {
+  if (!blue && (log_l < 0 || log_l > kMaxLogLReal)) {
     set_error("nfft=%d: fused kernels need a power of two <= %d (stft/spectrogram: or any "
-              "nfft <= %d)", nfft, 1 << kMaxLogL, kBlueMaxN);
+              "nfft <= %d)", nfft, 1 << kMaxLogLReal, kBlueMaxN);
     return SP_ERR_UNSUPPORTED;
   }
   // the spectral correction applies to the constant detrend when the window's spectrum is

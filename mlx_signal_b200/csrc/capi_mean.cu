@@ -154,9 +154,10 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   int log_l = ilog2_exact(nfft);
   // welch with a non-power-of-two nfft: the Bluestein kernel on a power-of-two transform
   const bool blue = log_l < 0 && !cplx && nfft >= 3 && nfft <= kBlueMaxN;
-  if (!blue && (log_l < 0 || log_l > kMaxLog)) {
+  const int max_log = cplx ? kMaxLog : kMaxLogLReal;
+  if (!blue && (log_l < 0 || log_l > max_log)) {
     set_error("nfft=%d: fused kernels need a power of two <= %d (or any nfft <= %d)",
-              nfft, 1 << kMaxLog, kBlueMaxN);
+              nfft, 1 << max_log, kBlueMaxN);
     return SP_ERR_UNSUPPORTED;
   }
   if (blue) log_l = blue_log_m(nfft);
@@ -396,7 +397,7 @@ int sp_csd_cplx(const float* x, const float* y, int64_t rows, int64_t n, int64_t
 
 int sp_welch_spectral_bins(int nfft) {
   const int log_l = b2s::ilog2_exact(nfft);
-  if (log_l < 1 || log_l > b2s::kMaxLog) return 0;
+  if (log_l < 1 || log_l > b2s::kMaxLogLReal) return 0;
   return b2s::spectral_bins(log_l);
 }
 

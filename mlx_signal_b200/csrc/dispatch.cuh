@@ -30,6 +30,9 @@ constexpr int batch_log_e() {
 }
 
 constexpr int kMaxLogL = 12;
+// The real-input segment-mean and per-frame families (welch, csd, coherence, stft,
+// spectrogram) also take nfft = 2^13: one 512-thread team per CTA (16 points per thread).
+constexpr int kMaxLogLReal = 13;
 
 // Runtime twin of team_log_e.
 inline int team_log_e_rt(int log_l) {
@@ -57,6 +60,7 @@ IstftInfo istft_half_lookup(int log_l);  // hop == nperseg / 2
 IstftInfo istft_cplx_lookup(int log_l);  // two-sided input, complex output
 
 // family: 0 welch mean, 1 cross mean
+// (log_l in [0, kMaxLogLReal] for the real-input families below)
 MeanInfo mean_lookup_welch(int log_l, int det);
 MeanInfo mean_lookup_cross(int log_l, int det);
 MeanInfo mean_lookup_welch_half(int log_l, int det);  // det 0/1/2(spectral), log_l >= 1
@@ -99,9 +103,9 @@ INFO lookup_seq(int log_l, int det, std::integer_sequence<int, LS...>) {
   return out;
 }
 
-template <class INFO, template <int, int> class F>
+template <class INFO, template <int, int> class F, int MAXL = kMaxLogL>
 INFO lookup_all(int log_l, int det) {
-  return lookup_seq<INFO, F>(log_l, det, std::make_integer_sequence<int, kMaxLogL + 1>{});
+  return lookup_seq<INFO, F>(log_l, det, std::make_integer_sequence<int, MAXL + 1>{});
 }
 
 }  // namespace b2s

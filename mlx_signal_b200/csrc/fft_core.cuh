@@ -215,18 +215,28 @@ constexpr TwMaster make_tw_master() {
 }
 static __device__ const TwMaster g_tw_master = make_tw_master();
 
-// Fill the twiddle tables of a plan (all passes) into shared memory from the master table.
+// Fill the twiddle tables of a plan (all passes) into shared memory: passes whose twiddles are
+// all entries of the master table gather them from it; a longer pass (L = 8192) evaluates its
+// entries with FP64 sincospi of the exactly reduced integer phase, rounded to FP32 once.
 template <class PL>
 __device__ void build_twiddles(float2* tw, int tid, int nthreads) {
-  static_assert(PL::L <= kTwMasterN, "plan longer than the master twiddle table");
   static_for<1, PL::NPASS>([&](auto pc) {
     constexpr int p = decltype(pc)::value;
     constexpr int R = PL::radix(p), S = PL::span(p), SR = S * R;
-    constexpr int step = kTwMasterN / SR;
     float2* t = tw + PL::tw_off(p);
-    for (int e = tid; e < R * S; e += nthreads) {
-      const int q = e / S, k = e - q * S;
-      t[e] = g_tw_master.v[((k * q) & (SR - 1)) * step];
+    if constexpr (SR <= kTwMasterN) {
+      constexpr int step = kTwMasterN / SR;
+      for (int e = tid; e < R * S; e += nthreads) {
+        const int q = e / S, k = e - q * S;
+        t[e] = g_tw_master.v[((k * q) & (SR - 1)) * step];
+      }
+    } else {
+      for (int e = tid; e < R * S; e += nthreads) {
+        const int q = e / S, k = e - q * S;
+        double sn, cs;
+        sincospi(-2.0 * double((k * q) & (SR - 1)) / double(SR), &sn, &cs);
+        t[e] = make_float2(float(cs), float(sn));
+      }
     }
   });
 }

@@ -21,6 +21,6 @@ struct F {
 };
 }  // namespace
 
-FrameInfo frame_lookup_cross(int log_l, int det) { return lookup_all<FrameInfo, F>(log_l, det); }
+FrameInfo frame_lookup_cross(int log_l, int det) { return lookup_all<FrameInfo, F, kMaxLogLReal>(log_l, det); }
 
 }  // namespace b2s

@@ -29,6 +29,6 @@ struct F {
 };
 }  // namespace
 
-FrameInfo frame_half_lookup_stft(int log_l, int det) { return lookup_all<FrameInfo, F>(log_l, det); }
+FrameInfo frame_half_lookup_stft(int log_l, int det) { return lookup_all<FrameInfo, F, kMaxLogLReal>(log_l, det); }
 
 }  // namespace b2s

@@ -21,7 +21,7 @@ struct F {
 };
 }  // namespace
 
-FrameInfo frame_lookup_stft(int log_l, int det) { return lookup_all<FrameInfo, F>(log_l, det); }
+FrameInfo frame_lookup_stft(int log_l, int det) { return lookup_all<FrameInfo, F, kMaxLogLReal>(log_l, det); }
 
 namespace {
 // constant detrend as a low-bin spectral correction (DET = kDetrendConstantSpectral)
@@ -44,6 +44,6 @@ struct FS {
 };
 }  // namespace
 
-FrameInfo frame_lookup_stft_spectral(int log_l) { return lookup_all<FrameInfo, FS>(log_l, 0); }
+FrameInfo frame_lookup_stft_spectral(int log_l) { return lookup_all<FrameInfo, FS, kMaxLogLReal>(log_l, 0); }
 
 }  // namespace b2s

@@ -28,8 +28,8 @@ struct Mode {
 }  // namespace
 
 MeanInfo mean_lookup_cross_half(int log_l, int det, bool csd) {
-  return csd ? lookup_all<MeanInfo, Mode<true>::F>(log_l, det)
-             : lookup_all<MeanInfo, Mode<false>::F>(log_l, det);
+  return csd ? lookup_all<MeanInfo, Mode<true>::F, kMaxLogLReal>(log_l, det)
+             : lookup_all<MeanInfo, Mode<false>::F, kMaxLogLReal>(log_l, det);
 }
 
 }  // namespace b2s

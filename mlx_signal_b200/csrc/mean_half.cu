@@ -25,6 +25,6 @@ struct F {
 };
 }  // namespace
 
-MeanInfo mean_lookup_welch_half(int log_l, int det) { return lookup_all<MeanInfo, F>(log_l, det); }
+MeanInfo mean_lookup_welch_half(int log_l, int det) { return lookup_all<MeanInfo, F, kMaxLogLReal>(log_l, det); }
 
 }  // namespace b2s

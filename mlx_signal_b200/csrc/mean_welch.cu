@@ -21,6 +21,6 @@ struct F {
 };
 }  // namespace
 
-MeanInfo mean_lookup_welch(int log_l, int det) { return lookup_all<MeanInfo, F>(log_l, det); }
+MeanInfo mean_lookup_welch(int log_l, int det) { return lookup_all<MeanInfo, F, kMaxLogLReal>(log_l, det); }
 
 }  // namespace b2s

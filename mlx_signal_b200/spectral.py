@@ -6,15 +6,16 @@ NumPy arrays, lists or torch tensors (CPU or CUDA); results are torch CUDA tenso
 complex64). Computation is float32/complex64.
 
 Routing (the reference's `_stft_metal.eligible` rule, spectral.py:319-347, widened): real
-float32 input with a power-of-two nfft <= 4096 and detrend in {False, 'constant', 'linear'}
+float32 input with a power-of-two nfft <= 8192 and detrend in {False, 'constant', 'linear'}
 runs the fused CUDA kernels (segment gather + detrend + window + FFT + |X|^2 or X conj(Y) +
 segment mean in one sweep); any other nfft <= 2048 runs fused Bluestein (chirp-z) kernels, and
-welch / stft / spectrogram of complex input (power-of-two nfft) the two-sided complex-input
-kernels (csd of two signals either of which is complex: the complex cross kernel), median
-averaging the per-frame kernels plus a column-median kernel. Other shapes (larger
-non-power-of-two nfft) run the composed GPU path: strided frames, torch elementwise ops and
-cuFFT -- the counterpart of the reference's composed MLX path (spectral.py:127-147). Nothing runs
-on the CPU.
+welch / stft / spectrogram of complex input (power-of-two nfft <= 4096) the two-sided
+complex-input kernels (csd of two signals either of which is complex: the complex cross
+kernel), median averaging the per-frame kernels plus a column-median kernel. istft of one- or
+two-sided spectra with a power-of-two nfft <= 4096 (frames of any nperseg <= nfft) is one fused
+kernel. Other shapes (longer non-power-of-two nfft) run the composed GPU path: strided frames,
+torch elementwise ops and cuFFT -- the counterpart of the reference's composed MLX path
+(spectral.py:127-147) -- and say so with a FallbackWarning. Nothing runs on the CPU.
 """
 
 from __future__ import annotations
@@ -367,9 +368,9 @@ def _setup(x, y, fs, window, nperseg, noverlap, nfft, detrend, return_onesided, 
     # non-power-of-two nfft <= 2048: Bluestein (chirp-z) kernels
     s.blue = (not x_complex) and (not y_complex) and _kernels.blue_ok(nfft)
     # complex input (same signal), power-of-two nfft: the two-sided complex-input kernels
-    s.cplx = x_complex and same and _kernels.fused_mean_ok(nfft)
+    s.cplx = x_complex and same and _kernels.fused_complex_ok(nfft)
     # csd of two signals, either complex, power-of-two nfft: the complex cross kernel
-    s.cplx2 = (not same) and (x_complex or y_complex) and _kernels.fused_mean_ok(nfft)
+    s.cplx2 = (not same) and (x_complex or y_complex) and _kernels.fused_complex_ok(nfft)
     return s
 
 

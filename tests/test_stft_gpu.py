@@ -537,3 +537,19 @@ def test_istft_two_sided_complex_fused(rng, kw):
         _, x2 = msig.istft(z, input_onesided=False, **kw)
     assert x2.is_complex() and x_ref.shape == tuple(x2.shape)
     assert_close(x2, x_ref)
+
+
+@pytest.mark.parametrize("kw", [{"nperseg": 8192}, {"nperseg": 8192, "noverlap": 6000},
+                                {"nperseg": 8192, "detrend": "constant"}])
+def test_stft_spectrogram_nfft_8192_fused(rng, kw):
+    import warnings
+
+    x = make_sig(rng, (2, 1 << 16))
+    _, _, z_ref = sps.stft(x.astype(np.float64), **kw)
+    _, _, s_ref = sps.spectrogram(x.astype(np.float64), window="hann", **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", msig.FallbackWarning)
+        _, _, z = msig.stft(x, **kw)
+        _, _, s = msig.spectrogram(x, window="hann", **kw)
+    assert_close(z, z_ref)
+    assert_close(s, s_ref)

@@ -500,3 +500,42 @@ def test_welch_long_channel_segment_sums():
     xh = x.cpu().numpy()
     _, pref = _welch_f64_chunked(xh, 256)
     assert rel_err_bins(p.cpu().numpy(), pref) <= 1e-5
+
+
+@pytest.mark.parametrize("kw", [
+    {"nperseg": 8192},
+    {"nperseg": 8192, "detrend": "linear"},
+    {"nperseg": 8192, "detrend": False, "window": "hamming"},
+    {"nperseg": 8192, "noverlap": 2048},
+    {"nperseg": 6000, "nfft": 8192},
+    {"nperseg": 8192, "average": "median"},
+])
+def test_welch_nfft_8192_fused(rng, kw):
+    """nfft = 8192 runs the fused kernels (one 512-thread team per CTA), no composed path."""
+    import warnings
+
+    x = make_sig(rng, (3, 1 << 17))
+    _, p_ref = sps.welch(x.astype(np.float64), **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", msig.FallbackWarning)
+        _, p = msig.welch(x, **kw)
+    assert_close(p, p_ref)
+    if kw.get("average") != "median":
+        assert rel_err_bins(p, p_ref) <= 1e-5
+
+
+@pytest.mark.parametrize("noverlap", [None, 1000])
+def test_csd_coherence_nfft_8192_fused(rng, noverlap):
+    import warnings
+
+    x = make_sig(rng, (2, 1 << 17))
+    y = 0.6 * np.roll(x, 9, axis=-1) + 0.4 * make_sig(rng, (2, 1 << 17))
+    kw = {"nperseg": 8192, "noverlap": noverlap}
+    _, c_ref = sps.csd(x.astype(np.float64), y.astype(np.float64), **kw)
+    _, h_ref = sps.coherence(x.astype(np.float64), y.astype(np.float64), **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", msig.FallbackWarning)
+        _, c = msig.csd(x, y, **kw)
+        _, h = msig.coherence(x, y, **kw)
+    assert_close(c, c_ref, rtol=2e-4)
+    assert_close(h, h_ref, rtol=1e-3)
