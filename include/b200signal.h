@@ -64,7 +64,7 @@ SP_API int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int npe
 /*
  * Welch PSD: out[r][k] = (onesided ? f_k : 1) / nseg * sum_s |FFT_nfft(win * detrend(x_rs))_k|^2
  * for k < (onesided ? nfft/2+1 : nfft), segments x_rs = x[r, s*hop : s*hop+nperseg].
- * nfft: a power of two in [1, 4096], or any other value in [3, 2048] (chirp-z kernels), with
+ * nfft: a power of two in [1, 8192], or any other value in [3, 4096] (chirp-z kernels), with
  * nperseg <= nfft; win holds nperseg values.
  * Replaces _stft_metal.rfft_power_mean (_stft_metal.py:530-557) together with the deferred
  * one-sided factor of spectral.csd (spectral.py:468-488); for a non-power-of-two nfft the composed

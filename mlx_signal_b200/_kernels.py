@@ -40,7 +40,7 @@ def fused_complex_ok(nfft: int) -> bool:
 
 
 #: longest non-power-of-two nfft the Bluestein kernels take (welch, stft, spectrogram)
-MAX_BLUE_NFFT = 2048
+MAX_BLUE_NFFT = 4096
 
 
 def blue_ok(nfft: int) -> bool:

@@ -27,6 +27,6 @@ struct F {
 };
 }  // namespace
 
-MeanInfo blue_lookup_cross(int log_m, int det) { return lookup_all<MeanInfo, F>(log_m, det); }
+MeanInfo blue_lookup_cross(int log_m, int det) { return lookup_all<MeanInfo, F, kMaxLogLReal>(log_m, det); }
 
 }  // namespace b2s

@@ -28,7 +28,7 @@ struct F {
 }  // namespace
 
 FrameInfo blue_lookup_frames_power(int log_m, int det) {
-  return lookup_all<FrameInfo, F>(log_m, det);
+  return lookup_all<FrameInfo, F, kMaxLogLReal>(log_m, det);
 }
 
 }  // namespace b2s

@@ -1,4 +1,4 @@
-// Instantiations of k_blue_welch (non-power-of-two nfft) for transform lengths 2^4..2^12 and
+// Instantiations of k_blue_welch (non-power-of-two nfft) for transform lengths 2^4..2^13 and
 // detrend none / constant / linear.
 #include "dispatch.cuh"
 
@@ -27,6 +27,6 @@ struct F {
 };
 }  // namespace
 
-MeanInfo blue_lookup_welch(int log_m, int det) { return lookup_all<MeanInfo, F>(log_m, det); }
+MeanInfo blue_lookup_welch(int log_m, int det) { return lookup_all<MeanInfo, F, kMaxLogLReal>(log_m, det); }
 
 }  // namespace b2s

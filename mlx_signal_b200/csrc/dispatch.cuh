@@ -71,8 +71,8 @@ FrameInfo frame_lookup_stft_spectral(int log_l);   // constant detrend, spectral
 FrameInfo frame_lookup_power_spectral(int log_l);
 FrameInfo frame_lookup_cross(int log_l, int det);
 // Bluestein kernels for a non-power-of-two nfft in [3, kBlueMaxN]: transform length
-// M = 2^log_m >= 2 nfft - 1 (log_m in [4, 12]); det 0 none, 1 constant, 2 linear.
-constexpr int kBlueMaxN = 2048;
+// M = 2^log_m >= 2 nfft - 1 (log_m in [4, 13]); det 0 none, 1 constant, 2 linear.
+constexpr int kBlueMaxN = 4096;
 inline int blue_log_m(int nfft) {
   int lm = 4;
   while ((1 << lm) < 2 * nfft - 1) ++lm;

@@ -8,7 +8,7 @@ complex64). Computation is float32/complex64.
 Routing (the reference's `_stft_metal.eligible` rule, spectral.py:319-347, widened): real
 float32 input with a power-of-two nfft <= 8192 and detrend in {False, 'constant', 'linear'}
 runs the fused CUDA kernels (segment gather + detrend + window + FFT + |X|^2 or X conj(Y) +
-segment mean in one sweep); any other nfft <= 2048 runs fused Bluestein (chirp-z) kernels, and
+segment mean in one sweep); any other nfft <= 4096 runs fused Bluestein (chirp-z) kernels, and
 welch / stft / spectrogram of complex input (power-of-two nfft <= 4096) the two-sided
 complex-input kernels (csd of two signals either of which is complex: the complex cross
 kernel), median averaging the per-frame kernels plus a column-median kernel. istft of one- or

@@ -58,7 +58,8 @@ def test_fused_routing_rule():
     assert _kernels.fused_mean_ok(8192) and not _kernels.fused_mean_ok(16384)
     assert not _kernels.fused_mean_ok(100) and not _kernels.fused_complex_ok(8192)
     assert _kernels.blue_ok(1000) and _kernels.blue_ok(3) and _kernels.blue_ok(2047)
-    assert not _kernels.blue_ok(1024) and not _kernels.blue_ok(2049)
+    assert _kernels.blue_ok(2049) and _kernels.blue_ok(4095)
+    assert not _kernels.blue_ok(1024) and not _kernels.blue_ok(4097)
 
 
 def test_config_validation_and_context():

@@ -539,3 +539,21 @@ def test_csd_coherence_nfft_8192_fused(rng, noverlap):
         _, h = msig.coherence(x, y, **kw)
     assert_close(c, c_ref, rtol=2e-4)
     assert_close(h, h_ref, rtol=1e-3)
+
+
+@pytest.mark.parametrize("kw", [{"nperseg": 3000}, {"nperseg": 4000, "detrend": "linear"},
+                                {"nperseg": 2500, "nfft": 3500}])
+def test_bluestein_long_nfft_fused(rng, kw):
+    """Non-power-of-two nfft in (2048, 4096]: the chirp-z kernels on 8192-point transforms."""
+    import warnings
+
+    x = make_sig(rng, (2, 1 << 16))
+    _, p_ref = sps.welch(x.astype(np.float64), **kw)
+    _, _, z_ref = sps.stft(x[0].astype(np.float64), **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", msig.FallbackWarning)
+        _, p = msig.welch(x, **kw)
+        _, _, z = msig.stft(x[0], **kw)
+    assert_close(p, p_ref)
+    assert rel_err_bins(p, p_ref) <= 1e-5
+    assert_close(z, z_ref)
