@@ -305,6 +305,18 @@ SP_API int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t l
 SP_API int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, int64_t n,
                         void* workspace, size_t workspace_bytes, void* stream);
 
+/*
+ * Analytic signal (scipy.signal.hilbert) of `batch` contiguous rows of n real float32 samples:
+ * out (batch, n) complex64 = IFFT_n(h FFT_n(x)) with h = 1 at 0 and n/2, 2 between, 0 above.
+ * n even with n/2 and n powers of two in [2^12, 2^26]; workspace sp_fft_workspace_size(n, batch)
+ * bytes (same error word as sp_fft_c64). Forward packed real transform (three passes), one
+ * kernel that untangles it and writes the masked spectrum into `out`, and the n-point inverse
+ * transform in place. Replaces the reference's hilbert (filtering.py:43-84: rfft, mask, ifft as
+ * separate array operations).
+ */
+SP_API int sp_hilbert_c64(const float* x, float* out, int batch, int64_t n, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
 /* Byte offset of the int error word inside a long-transform workspace (0 = ok, SP_ERR_TIMEOUT if
  * a tile copy wait gave up); read it after synchronising the stream. */
 SP_API int sp_fft_error_word(const void* workspace, int64_t n, int batch, int64_t* offset);

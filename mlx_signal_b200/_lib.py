@@ -109,6 +109,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "sp_irfft_f32": (c_i, [c_fp, c_i64, c_i, c_fp, c_i, c_i64, c_p, c_sz, c_p]),
     "sp_fft_error_word": (c_i, [c_p, c_i64, c_i, ctypes.POINTER(c_i64)]),
     "sp_fft_set_wait_limit": (ctypes.c_uint32, [ctypes.c_uint32]),
+    "sp_hilbert_c64": (c_i, [c_fp, c_fp, c_i, c_i64, c_p, c_sz, c_p]),
     "sp_dft32_tc_c64": (c_i, [c_fp, c_fp, c_i64, c_i, c_p, c_p]),
     "sp_conv_ols_f32": (c_i, [c_fp, c_i64, c_i64, c_i64, c_fp, c_i, c_i64, c_i64, c_fp, c_i64,
                               c_p]),

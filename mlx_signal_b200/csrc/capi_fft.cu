@@ -240,6 +240,42 @@ int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t ldx_out,
   return SP_OK;
 }
 
+int sp_hilbert_c64(const float* x, float* out, int batch, int64_t n, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  using namespace b2s;
+  int e;
+  if (n % 2) {
+    set_error("sp_hilbert_c64: n must be even");
+    return SP_ERR_UNSUPPORTED;
+  }
+  const int64_t m = n / 2;
+  int st = check_n(m, &e);
+  if (st != SP_OK) return st;
+  int en;
+  if ((st = check_n(n, &en)) != SP_OK) return st;
+  if (!x || !out || !workspace || batch < 1 || !aligned16(x) || !aligned16(out) ||
+      !aligned16(workspace)) {
+    set_error("sp_hilbert_c64: null or misaligned (16 B) pointer, or batch < 1");
+    return SP_ERR_ARG;
+  }
+  if (int64_t(workspace_bytes) < ws_need(n, batch)) {
+    set_error("workspace too small: need %lld bytes", (long long)ws_need(n, batch));
+    return SP_ERR_WORKSPACE;
+  }
+  auto s = static_cast<cudaStream_t>(stream);
+  float2* s1 = static_cast<float2*>(workspace);
+  float2* s2 = s1 + int64_t(batch) * n;
+  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * n);
+  B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
+  float2* y = reinterpret_cast<float2*>(out);
+  // packed m-point transform of the n reals (Z in s1), the analytic spectrum into `out`, then
+  // the n-point inverse transform of `out` in place (pass 1 reads it before pass 3 writes it)
+  if ((st = fft3(reinterpret_cast<const float2*>(x), s1, s2, s1, batch, e, 0, err, s))) return st;
+  k_hilbert_spectrum<<<untangle_blocks(m, batch), kUntB, 0, s>>>(s1, y, m, untangle_step(m));
+  B2S_CHECK_CUDA(cudaGetLastError(), "hilbert spectrum launch");
+  return fft3(y, s1, s2, y, batch, en, 1, err, s);
+}
+
 int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, int64_t n,
                  void* workspace, size_t workspace_bytes, void* stream) {
   using namespace b2s;

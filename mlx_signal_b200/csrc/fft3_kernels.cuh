@@ -356,6 +356,58 @@ __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restric
   }
 }
 
+// Analytic-signal spectrum of n = 2m real samples from the packed transform Z = FFT_m(z)
+// (scipy.signal.hilbert's mask h for even n): the untangle above gives X_k for k <= m, and
+//   Y_0 = X_0, Y_k = 2 X_k (0 < k < m), Y_m = X_m, Y_k = 0 (m < k < 2m)
+// is written as the input of the n-point inverse FFT (row stride 2m complex). Index k in
+// [0, m/2] writes Y_k, Y_{m-k} and the zeros Y_{m+k}, Y_{2m-k}.
+__global__ void __launch_bounds__(kUntB) k_hilbert_spectrum(const float2* __restrict__ Z,
+                                                            float2* __restrict__ Y, int64_t m,
+                                                            double2 d) {
+  const int64_t half = m / 2 + 1;
+  const int64_t per_row = (half + kUntB * kUntT - 1) / (kUntB * kUntT);
+  const int64_t b = blockIdx.x / per_row;
+  const int64_t k0 = (blockIdx.x - b * per_row) * (kUntB * kUntT) + threadIdx.x;
+  const float2* z = Z + b * m;
+  float2* y = Y + b * 2 * m;
+  float2 zks[kUntT], zms[kUntT];
+#pragma unroll
+  for (int j = 0; j < kUntT; ++j) {
+    const int64_t k = k0 + int64_t(j) * kUntB;
+    zks[j] = k < half ? z[k] : make_float2(0.f, 0.f);
+    zms[j] = (k < half && k != 0) ? z[m - k] : make_float2(0.f, 0.f);
+  }
+  double sn, cs;
+  sincospi(-double(k0) / double(m), &sn, &cs);
+  double2 w = make_double2(cs, sn);
+  const float2 zero = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int j = 0; j < kUntT; ++j) {
+    const int64_t k = k0 + int64_t(j) * kUntB;
+    if (k < half) {
+      if (k == 0) {
+        const float2 z0 = zks[j];
+        y[0] = make_float2(z0.x + z0.y, 0.f);
+        y[m] = make_float2(z0.x - z0.y, 0.f);
+      } else {
+        const float2 zk = zks[j], zm = zms[j];
+        const float2 wf = make_float2(float(w.x), float(w.y));
+        const float2 ze = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 zo = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));
+        const float2 wz = cmul(wf, zo);
+        y[k] = make_float2(2.f * (ze.x + wz.y), 2.f * (ze.y - wz.x));
+        y[m + k] = zero;
+        if (2 * k != m) {
+          const float2 wz2 = make_float2(wz.x, -wz.y);
+          y[m - k] = make_float2(2.f * (ze.x + wz2.y), 2.f * (-ze.y - wz2.x));
+          y[2 * m - k] = zero;
+        }
+      }
+    }
+    w = zmul(w, d);
+  }
+}
+
 // Inverse of the untangle (irfft pre-twist): from X_0..X_m build the packed spectrum
 //   Y_k = E_k + i conj(w_k) O_k, E = (X_k + conj X_{m-k})/2, O = (X_k - conj X_{m-k})/2,
 // with X_0, X_m taken as real; then z = IFFT_m(Y) interleaves the n real samples.

@@ -28,6 +28,28 @@ def test_hilbert_matches_scipy(rng, n, N):
     assert peak_err(got, ref) < 2e-6
 
 
+@pytest.mark.parametrize("n,shape_axis", [(1 << 13, ((3, 1 << 13), -1)),
+                                         (1 << 14, ((1 << 14, 2), 0)),
+                                         (1 << 16, ((1, 1 << 16), -1))])
+def test_hilbert_fused_chain(rng, monkeypatch, n, shape_axis):
+    """Power-of-two lengths run sp_hilbert_c64 (forward three-pass transform, masked-spectrum
+    untangle, inverse three-pass transform); the kernels are routed from 2^12 points here."""
+    from mlx_signal_b200 import fft as bfft
+
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
+    shape, axis = shape_axis
+    x = rng.standard_normal(shape).astype(np.float32)
+    ref = sps.hilbert(x.astype(np.float64), axis=axis)
+    got = msig.hilbert(x, axis=axis)
+    assert bfft.device_status() == 0
+    assert tuple(got.shape) == ref.shape
+    assert peak_err(got, ref) < 2e-6
+    # the analytic signal of a cosine is the complex exponential
+    t = np.arange(n)
+    c = np.cos(2 * np.pi * 37 * t / n).astype(np.float32)
+    assert peak_err(msig.hilbert(c), np.exp(2j * np.pi * 37 * t / n)) < 2e-6
+
+
 def test_hilbert_axis_and_errors(rng):
     x = rng.standard_normal((4096, 3)).astype(np.float32)
     assert peak_err(msig.hilbert(x, axis=0), sps.hilbert(x.astype(np.float64), axis=0)) < 2e-6
