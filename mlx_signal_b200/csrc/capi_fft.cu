@@ -61,6 +61,24 @@ int make_map(CUtensorMap* map, const void* base, int64_t d0, int64_t d1, int64_t
   return SP_OK;
 }
 
+// Launch as a programmatic dependent of the stream's previous kernel (the kernels call
+// griddepcontrol.wait before reading anything that kernel may write).
+template <class K, class... Args>
+cudaError_t launch_pdl(K kernel, dim3 grid, int threads, size_t smem, cudaStream_t s,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(unsigned(threads));
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // points per thread of the tile-column FFT of length 2^LOG_L
 template <int LOG_L>
 constexpr int fft3_log_e() {
@@ -82,8 +100,8 @@ int launch_one(const CUtensorMap& map, Fft3Params p, int tiles, cudaStream_t s) 
   }
   p.ntiles = tiles;
   const int grid = tiles < nb * sms ? tiles : nb * sms;
-  k<<<grid, CFG::THREADS, kSmem, s>>>(map, p);
-  B2S_CHECK_CUDA(cudaGetLastError(), "fft3 pass launch");
+  B2S_CHECK_CUDA(launch_pdl(k, dim3(unsigned(grid)), CFG::THREADS, kSmem, s, map, p),
+                 "fft3 pass launch");
   return SP_OK;
 }
 
@@ -234,9 +252,10 @@ int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t ldx_out,
   B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
   // the n real samples are m interleaved complex values; Z lands in s1 (free after pass 2)
   if ((st = fft3(reinterpret_cast<const float2*>(x), s1, s2, s1, batch, e, 0, err, s))) return st;
-  k_rfft_untangle<<<untangle_blocks(m, batch), kUntB, 0, s>>>(
-      s1, reinterpret_cast<float2*>(X), m, ldx_out, untangle_step(m));
-  B2S_CHECK_CUDA(cudaGetLastError(), "rfft untangle launch");
+  B2S_CHECK_CUDA(launch_pdl(k_rfft_untangle, dim3(untangle_blocks(m, batch)), kUntB, 0, s,
+                            static_cast<const float2*>(s1), reinterpret_cast<float2*>(X), m,
+                            ldx_out, untangle_step(m)),
+                 "rfft untangle launch");
   return SP_OK;
 }
 
@@ -271,8 +290,9 @@ int sp_hilbert_c64(const float* x, float* out, int batch, int64_t n, void* works
   // packed m-point transform of the n reals (Z in s1), the analytic spectrum into `out`, then
   // the n-point inverse transform of `out` in place (pass 1 reads it before pass 3 writes it)
   if ((st = fft3(reinterpret_cast<const float2*>(x), s1, s2, s1, batch, e, 0, err, s))) return st;
-  k_hilbert_spectrum<<<untangle_blocks(m, batch), kUntB, 0, s>>>(s1, y, m, untangle_step(m));
-  B2S_CHECK_CUDA(cudaGetLastError(), "hilbert spectrum launch");
+  B2S_CHECK_CUDA(launch_pdl(k_hilbert_spectrum, dim3(untangle_blocks(m, batch)), kUntB, 0, s,
+                            static_cast<const float2*>(s1), y, m, untangle_step(m)),
+                 "hilbert spectrum launch");
   return fft3(y, s1, s2, y, batch, en, 1, err, s);
 }
 
@@ -301,9 +321,10 @@ int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, in
   float2* s2 = s1 + int64_t(batch) * m;
   int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * m);
   B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
-  k_irfft_pretwist<<<untangle_blocks(m, batch), kUntB, 0, s>>>(
-      reinterpret_cast<const float2*>(X), ldx, nbins, s2, m, untangle_step(m));
-  B2S_CHECK_CUDA(cudaGetLastError(), "irfft pretwist launch");
+  B2S_CHECK_CUDA(launch_pdl(k_irfft_pretwist, dim3(untangle_blocks(m, batch)), kUntB, 0, s,
+                            reinterpret_cast<const float2*>(X), ldx, nbins, s2, m,
+                            untangle_step(m)),
+                 "irfft pretwist launch");
   // Y (in s2) -> S1 (s1) -> S2 (s2, Y already consumed by pass 1) -> x
   return fft3(s2, s1, s2, reinterpret_cast<float2*>(x), batch, e, 1, err, s);
 }

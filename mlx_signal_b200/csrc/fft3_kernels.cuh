@@ -47,6 +47,16 @@ struct Fft3Params {
   uint32_t wait_polls; // poll limit of the wait for each tile's copy (kMbarSpinLimit by default)
 };
 
+// Programmatic dependent launch: the passes and the untangle kernels are launched as dependents
+// of the stream's previous kernel; each builds what needs no input, waits for the previous grid
+// to complete, then lets its own dependent start its prologue.
+__device__ __forceinline__ void fft_pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void fft_pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 constexpr int kTileCols = 16;                  // columns per tile: 16 complex = 128 B rows
 constexpr uint32_t kMbarSpinLimit = 1u << 22;  // bounded mbarrier polling
 
@@ -181,6 +191,8 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
   }
   build_twiddles<PL>(tw, threadIdx.x, blockDim.x);
   __syncthreads();
+  fft_pdl_wait();  // the previous pass (or kernel) has completed: its output may be read
+  fft_pdl_trigger();
   auto issue = [&](int tl, int j) {  // thread 0: TMA load of tile tl into buffer j
     int cg_, slab_, b_;
     fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg_, &slab_, &b_);
@@ -312,6 +324,8 @@ constexpr int kUntT = 8;    // indices per thread
 __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restrict__ Z,
                                                          float2* __restrict__ X, int64_t m,
                                                          int64_t ldx, double2 d) {
+  fft_pdl_wait();
+  fft_pdl_trigger();
   const int64_t half = m / 2 + 1;
   const int64_t per_row = (half + kUntB * kUntT - 1) / (kUntB * kUntT);
   const int64_t b = blockIdx.x / per_row;
@@ -364,6 +378,8 @@ __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restric
 __global__ void __launch_bounds__(kUntB) k_hilbert_spectrum(const float2* __restrict__ Z,
                                                             float2* __restrict__ Y, int64_t m,
                                                             double2 d) {
+  fft_pdl_wait();
+  fft_pdl_trigger();
   const int64_t half = m / 2 + 1;
   const int64_t per_row = (half + kUntB * kUntT - 1) / (kUntB * kUntT);
   const int64_t b = blockIdx.x / per_row;
@@ -415,6 +431,8 @@ __global__ void __launch_bounds__(kUntB) k_irfft_pretwist(const float2* __restri
                                                           int64_t ldx, int nbins,
                                                           float2* __restrict__ Y, int64_t m,
                                                           double2 d) {
+  fft_pdl_wait();
+  fft_pdl_trigger();
   const int64_t half = m / 2 + 1;
   const int64_t per_row = (half + kUntB * kUntT - 1) / (kUntB * kUntT);
   const int64_t b = blockIdx.x / per_row;
