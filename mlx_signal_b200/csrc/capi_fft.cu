@@ -88,7 +88,8 @@ constexpr int fft3_log_e() {
 // Persistent launch: at most the resident CTAs (occupancy x SMs), each walking its share of
 // the pass's `tiles` (resident_ctas also raises the kernel's shared-memory limit per device).
 template <int PASS, int LL>
-int launch_one(const CUtensorMap& map, Fft3Params p, int tiles, cudaStream_t s) {
+int launch_one(const CUtensorMap& map, const CUtensorMap& omap, Fft3Params p, int tiles,
+               cudaStream_t s) {
   using CFG = Fft3Cfg<LL, fft3_log_e<LL>()>;
   auto k = &k_fft3_pass<LL, fft3_log_e<LL>(), PASS>;
   constexpr size_t kSmem = CFG::smem(PASS);
@@ -100,21 +101,22 @@ int launch_one(const CUtensorMap& map, Fft3Params p, int tiles, cudaStream_t s) 
   }
   p.ntiles = tiles;
   const int grid = tiles < nb * sms ? tiles : nb * sms;
-  B2S_CHECK_CUDA(launch_pdl(k, dim3(unsigned(grid)), CFG::THREADS, kSmem, s, map, p),
+  B2S_CHECK_CUDA(launch_pdl(k, dim3(unsigned(grid)), CFG::THREADS, kSmem, s, map, omap, p),
                  "fft3 pass launch");
   return SP_OK;
 }
 
 template <int PASS>
-int launch_pass(int log_l, const CUtensorMap& map, const Fft3Params& p, int blocks,
+int launch_pass(int log_l, const CUtensorMap& map, const CUtensorMap& omap, const Fft3Params& p,
+                int blocks,
                 cudaStream_t s) {  // blocks = tiles of the pass
   switch (log_l) {
-    case 4: return launch_one<PASS, 4>(map, p, blocks, s);
-    case 5: return launch_one<PASS, 5>(map, p, blocks, s);
-    case 6: return launch_one<PASS, 6>(map, p, blocks, s);
-    case 7: return launch_one<PASS, 7>(map, p, blocks, s);
-    case 8: return launch_one<PASS, 8>(map, p, blocks, s);
-    case 9: return launch_one<PASS, 9>(map, p, blocks, s);
+    case 4: return launch_one<PASS, 4>(map, omap, p, blocks, s);
+    case 5: return launch_one<PASS, 5>(map, omap, p, blocks, s);
+    case 6: return launch_one<PASS, 6>(map, omap, p, blocks, s);
+    case 7: return launch_one<PASS, 7>(map, omap, p, blocks, s);
+    case 8: return launch_one<PASS, 8>(map, omap, p, blocks, s);
+    case 9: return launch_one<PASS, 9>(map, omap, p, blocks, s);
     default:
       set_error("unsupported pass length 2^%d", log_l);
       return SP_ERR_UNSUPPORTED;
@@ -138,7 +140,7 @@ int fft3(const float2* in, float2* s1, float2* s2, float2* out, int batch, int e
   p.ntiles = 0;
   p.wait_polls = g_wait_polls.load(std::memory_order_relaxed);
   const int l3 = ilog2_exact(R3), l2 = ilog2_exact(R2), l1 = ilog2_exact(R1);
-  CUtensorMap m1, m2, m3;
+  CUtensorMap m1, m2, m3, o2, o3;
   int st;
   // pass 1 source x[b][m3][m2][r]: dims {2 R1, R2, batch R3}, box {32, 1, min(R3, 256)}
   if ((st = make_map(&m1, in, R1, R2, int64_t(batch) * R3, 1, R3 < 256 ? R3 : 256))) return st;
@@ -146,15 +148,20 @@ int fft3(const float2* in, float2* s1, float2* s2, float2* out, int batch, int e
   if ((st = make_map(&m2, s1, R3, R1, int64_t(batch) * R2, 1, R2 < 256 ? R2 : 256))) return st;
   // pass 3 source S2[b][km2][r][km3]: dims {2 R3, R1, batch R2}, box {32, min(R1, 256), 1}
   if ((st = make_map(&m3, s2, R3, R1, int64_t(batch) * R2, R1 < 256 ? R1 : 256, 1))) return st;
+  // pass 2 destination S2 (TMA stores of row tiles): dims {2 R3, R1, batch R2},
+  // box {32, 1, min(R2, 256)}; pass 3 destination X[b][kr][km2][km3]: dims {2 R3, R2, batch R1},
+  // box {32, 1, min(R1, 256)}
+  if ((st = make_map(&o2, s2, R3, R1, int64_t(batch) * R2, 1, R2 < 256 ? R2 : 256))) return st;
+  if ((st = make_map(&o3, out, R3, R2, int64_t(batch) * R1, 1, R1 < 256 ? R1 : 256))) return st;
   p.in = in;
   p.out = s1;
-  if ((st = launch_pass<1>(l3, m1, p, batch * R2 * (R1 / kTileCols), s))) return st;
+  if ((st = launch_pass<1>(l3, m1, m1, p, batch * R2 * (R1 / kTileCols), s))) return st;
   p.in = s1;
   p.out = s2;
-  if ((st = launch_pass<2>(l2, m2, p, batch * R1 * (R3 / kTileCols), s))) return st;
+  if ((st = launch_pass<2>(l2, m2, o2, p, batch * R1 * (R3 / kTileCols), s))) return st;
   p.in = s2;
   p.out = out;
-  if ((st = launch_pass<3>(l1, m3, p, batch * R2 * (R3 / kTileCols), s))) return st;
+  if ((st = launch_pass<3>(l1, m3, o3, p, batch * R2 * (R3 / kTileCols), s))) return st;
   return SP_OK;
 }
 

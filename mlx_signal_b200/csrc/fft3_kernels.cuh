@@ -100,6 +100,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// 3-D tiled TMA store of one box from shared memory at coordinates {c0, c1, c2} (bulk group).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0,
+                                             int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
 // Element (row, col) of a tile whose 128-byte rows were written with the 128B swizzle: the
 // 16-byte chunk index is XORed with (row mod 8).
 __device__ __forceinline__ int swz(int row, int col) {
@@ -165,7 +175,8 @@ __device__ __forceinline__ void fft3_tile_coords(int tile, int R1, int R2, int R
 template <int LOG_L, int LOG_E, int PASS>
 __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
                                   Fft3Cfg<LOG_L, LOG_E>::min_blocks(PASS))
-    k_fft3_pass(const __grid_constant__ CUtensorMap src, Fft3Params pr) {
+    k_fft3_pass(const __grid_constant__ CUtensorMap src, const __grid_constant__ CUtensorMap dst,
+                Fft3Params pr) {
   using CFG = Fft3Cfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
   constexpr int L = PL::L, E = PL::E, P = PL::P;
@@ -216,7 +227,11 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
     const int j = it & 1;
     const uint32_t par = uint32_t(it >> 1) & 1u;
     const int nxt = tl + int(gridDim.x);
-    if (threadIdx.x == 0 && nxt < pr.ntiles) issue(nxt, j ^ 1);
+    if (threadIdx.x == 0 && nxt < pr.ntiles) {
+      // passes 2 and 3: the previous tile's TMA store must have read buffer j ^ 1 first
+      if constexpr (PASS != 1) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      issue(nxt, j ^ 1);
+    }
     // This tile's inter-pass twiddles, computed while its copy is in flight (the previous
     // tile's readers finished at the last barrier; the wait below publishes them). Each is an
     // independent FP64 sincospi of an exactly reduced integer phase, rounded once to FP32:
@@ -250,6 +265,7 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
         // write lands in this CTA's shared memory after it exits
         (void)mbar_wait(bar + j, par);
         if (nxt < pr.ntiles) (void)mbar_wait(bar + (j ^ 1), uint32_t((it + 1) >> 1) & 1u);
+        if constexpr (PASS != 1) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
       }
       return;
     }
@@ -293,22 +309,25 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
         if (PASS == 3 && pr.inverse) z.y = -z.y;
         tile[swz(t + e * P, c)] = z;
       }
+      // the staged tile (128-byte rows in the load's swizzle) goes out as TMA tensor stores:
+      //   PASS 2: S2[b][km2 = row][r = slab][km3 = col0 ..] at {2 col0, slab, b R2 + row},
+      //   PASS 3: X[b][kr = row][km2 = slab][km3 = col0 ..] at {2 col0, slab, b R1 + row}
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
-      // coalesced row stores: row k (L rows) holds 16 consecutive complex outputs
-      //   PASS 2: S2[b][km2 = k][r = slab][km3 = col0 ..], PASS 3: X[b][kr = k][km2 = slab][km3 ..]
-      const int64_t row_stride = PASS == 2 ? int64_t(R1) * R3 : int64_t(R2) * R3;
-      float2* dst = pr.out + int64_t(b) * N + int64_t(slab) * R3 + col0;
-      for (int i = threadIdx.x; i < L * (kTileCols / 2); i += blockDim.x) {
-        const int row = i / (kTileCols / 2), cp = (i % (kTileCols / 2)) * 2;
-        const float2 a0 = tile[swz(row, cp)];
-        const float2 a1 = tile[swz(row, cp + 1)];
-        *reinterpret_cast<float4*>(dst + row * row_stride + cp) = make_float4(a0.x, a0.y, a1.x, a1.y);
+      if (threadIdx.x == 0) {
+        for (int r0 = 0; r0 < L; r0 += 256)
+          tma_store_3d(&dst, tile + r0 * kTileCols, 2 * col0, slab, b * L + r0);
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
       }
     }
     // The slot was written through the generic proxy (exchange, output staging); order those
     // accesses before the TMA (async proxy) that refills it with tile it + 2.
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();  // slot j is free for the load of tile it + 2
+  }
+  // the last TMA stores complete before the CTA (and its shared memory) goes away
+  if constexpr (PASS != 1) {
+    if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 }
 
