@@ -255,11 +255,12 @@ SP_API int sp_istft_f32(const float* z, int64_t rows, int nseg, int64_t ld_row, 
                         float* out, void* stream);
 
 /*
- * sp_istft_f32 with an FFT length nfft >= nperseg (a power of two in [2, 4096]; any nperseg >= 1):
- * each frame is the first nperseg samples of the nfft-point inverse real FFT of its one-sided
- * spectrum (nbins_in <= nfft/2 + 1 bins), windowed by the nperseg-point win; outlen = nperseg +
- * (nseg-1)*hop. nfft == nperseg is sp_istft_f32. Replaces the composed zero-padded branch of
- * spectral.istft (spectral.py:929-950: irfft(n=nfft)[:nperseg], then overlap-add).
+ * sp_istft_f32 with an FFT length nfft >= nperseg (a power of two in [2, 4096], or any other
+ * value in [3, 2048]: chirp-z kernel; any nperseg >= 1): each frame is the first nperseg samples
+ * of the nfft-point inverse real DFT of its one-sided spectrum (nbins_in <= nfft/2 + 1 bins),
+ * windowed by the nperseg-point win; outlen = nperseg + (nseg-1)*hop. nfft == nperseg is
+ * sp_istft_f32. Replaces the composed branch of spectral.istft (spectral.py:929-950:
+ * irfft(n=nfft)[:nperseg], then overlap-add).
  */
 SP_API int sp_istft_f32_ex(const float* z, int64_t rows, int nseg, int64_t ld_row, int ldf,
                            int nbins_in, const float* win, float scale, int nperseg, int nfft,

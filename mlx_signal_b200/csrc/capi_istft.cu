@@ -15,15 +15,19 @@ int sp_istft_f32_ex(const float* z, int64_t rows, int nseg, int64_t ld_row, int 
               nseg, nperseg, nfft, hop, nbins_in, ldf);
     return SP_ERR_ARG;
   }
-  const int log_l = ilog2_exact(nfft);
-  if (log_l < 1 || log_l > kMaxLogL) {
-    set_error("nfft=%d: the fused istft needs a power of two in [2, %d]", nfft, 1 << kMaxLogL);
+  int log_l = ilog2_exact(nfft);
+  // a non-power-of-two nfft: the chirp-z kernel on a power-of-two transform
+  const bool blue = log_l < 0 && nfft >= 3 && nfft <= kBlueIstftMaxN;
+  if (!blue && (log_l < 1 || log_l > kMaxLogL)) {
+    set_error("nfft=%d: the fused istft needs a power of two in [2, %d] or any nfft in [3, %d]",
+              nfft, 1 << kMaxLogL, kBlueIstftMaxN);
     return SP_ERR_UNSUPPORTED;
   }
   if (rows == 0) return SP_OK;
   // register overlap-add (no ring buffer) for whole-length frames at half overlap
-  const bool half = nperseg == nfft && 2 * hop == nperseg;
-  const IstftInfo k = half ? istft_half_lookup(log_l) : istft_lookup(log_l);
+  const bool half = !blue && nperseg == nfft && 2 * hop == nperseg;
+  const IstftInfo k = blue ? istft_blue_lookup(blue_log_m(nfft))
+                           : (half ? istft_half_lookup(log_l) : istft_lookup(log_l));
   int sms = 0;
   const int nb = resident_ctas(k.fn, k.threads, k.smem, &sms);
   if (nb <= 0) {
@@ -41,6 +45,7 @@ int sp_istft_f32_ex(const float* z, int64_t rows, int nseg, int64_t ld_row, int 
   p.win = win;
   p.scale = scale;
   p.nper = nperseg;
+  p.nfft = nfft;
   p.outlen = int64_t(nperseg) + int64_t(nseg - 1) * hop;
   p.out = out;
   p.total = rows * nseg;
@@ -98,6 +103,7 @@ int sp_istft_c64(const float* z, int64_t rows, int nseg, int64_t ld_row, int ldf
   p.win = win;
   p.scale = scale;
   p.nper = nperseg;
+  p.nfft = nfft;
   p.outlen = int64_t(nperseg) + int64_t(nseg - 1) * hop;
   p.out = out;
   p.total = rows * nseg;

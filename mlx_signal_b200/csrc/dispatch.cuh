@@ -58,6 +58,8 @@ using IstftInfo = KernelInfo<IstftParams>;
 IstftInfo istft_lookup(int log_l);       // log_l in [1, kMaxLogL]
 IstftInfo istft_half_lookup(int log_l);  // hop == nperseg / 2
 IstftInfo istft_cplx_lookup(int log_l);  // two-sided input, complex output
+IstftInfo istft_blue_lookup(int log_m);  // non-power-of-two nfft <= kBlueIstftMaxN (chirp-z)
+constexpr int kBlueIstftMaxN = 2048;
 
 // family: 0 welch mean, 1 cross mean
 // (log_l in [0, kMaxLogLReal] for the real-input families below)

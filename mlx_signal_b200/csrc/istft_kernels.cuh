@@ -33,6 +33,7 @@ struct IstftParams {
   const float* win;  // nper window values
   float scale;       // istft scale (spectrum: sum(win); psd: sqrt(fs sum(win^2)))
   int nper;          // frame length (nperseg <= L): the first nper samples of each inverse FFT
+  int nfft;          // DFT length of the chirp-z (non-power-of-two) kernel; L for the others
   int64_t outlen;    // nper + (nseg - 1) * hop
   float* out;        // (rows, outlen)
   int64_t G;         // output frames owned per team

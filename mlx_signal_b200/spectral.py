@@ -879,9 +879,10 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
         raise ValueError(f"Parameter {scaling=} not in ['spectrum', 'psd']!")
     outputlength = nperseg + (nseg - 1) * nstep
     batch = Z.shape[:-2]
-    if _kernels.is_pow2(nfft) and 2 <= nfft <= _kernels.MAX_FUSED_NFFT:
-        # fused: one-sided (irfft) or two-sided (ifft, complex output) spectra, frames of
-        # nperseg <= nfft samples
+    if (_kernels.is_pow2(nfft) and 2 <= nfft <= _kernels.MAX_FUSED_NFFT) or \
+            (input_onesided and not _kernels.is_pow2(nfft) and 3 <= nfft <= 2048):
+        # fused: one-sided (irfft; a non-power-of-two nfft through the chirp-z kernel) or
+        # two-sided (ifft, complex output) spectra, frames of nperseg <= nfft samples
         plan = _IstftPlan(device_vector(win_np.astype(np.float32)), scale, nperseg, nstep,
                           batch, outputlength, bool(boundary),
                           _nola_ok(win_np, nperseg, nstep, nseg, outputlength, bool(boundary)),
@@ -891,7 +892,7 @@ def istft(Zxx, fs=1.0, window="hann", nperseg=None, noverlap=None, nfft=None,
                 _ISTFT_PLANS.clear()
             _ISTFT_PLANS[key] = plan
         return plan.run(Z, permuted=True)
-    composed_path_notice("istft", "non-power-of-two nfft (composed inverse path)")
+    composed_path_notice("istft", "nfft outside the fused kernels (composed inverse path)")
     if input_onesided:
         xsubs = torch.fft.irfft(Z, n=nfft, dim=-1)[..., :nperseg]
     else:

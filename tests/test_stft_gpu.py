@@ -553,3 +553,22 @@ def test_stft_spectrogram_nfft_8192_fused(rng, kw):
         _, _, s = msig.spectrogram(x, window="hann", **kw)
     assert_close(z, z_ref)
     assert_close(s, s_ref)
+
+
+@pytest.mark.parametrize("nperseg,nfft,noverlap", [(1000, None, 500), (300, None, 200),
+                                                  (100, 150, 60), (999, 1500, None),
+                                                  (37, None, 20)])
+def test_istft_non_power_of_two_fused(rng, nperseg, nfft, noverlap):
+    """A non-power-of-two nfft runs the chirp-z fused inverse (no composed-path warning)."""
+    import warnings
+
+    x = make_sig(rng, (2, 5000))
+    kw = dict(nperseg=nperseg, nfft=nfft, noverlap=noverlap)
+    _, _, z = sps.stft(x.astype(np.float64), **kw)
+    _, x_ref = sps.istft(z, **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error", msig.FallbackWarning)
+        warnings.simplefilter("ignore", msig.DowncastWarning)
+        _, x2 = msig.istft(z, **kw)
+    assert x_ref.shape == tuple(x2.shape)
+    assert_close(x2, x_ref)
