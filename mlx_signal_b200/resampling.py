@@ -15,7 +15,7 @@ import torch
 
 from . import fft as _fft
 from ._array import device, to_device, to_numpy
-from .windows import _window_np
+from .windows import _window_np, device_vector
 
 __all__ = ["resample"]
 
@@ -37,8 +37,17 @@ def _freq_window(window, n: int) -> np.ndarray:
 
 
 def _dev(vals: np.ndarray) -> torch.Tensor:
+    """A host vector on the device, uploaded once per (values, dtype) through the byte-budget
+    constant cache (a repeat call does no pageable, stream-synchronising upload)."""
     dt = torch.complex64 if np.iscomplexobj(vals) else torch.float32
-    return torch.from_numpy(np.ascontiguousarray(vals)).to(device(), dtype=dt)
+    return device_vector(np.ascontiguousarray(vals), dtype=dt)
+
+
+def _scale_bin(X: torch.Tensor, k: int, fac: float) -> torch.Tensor:
+    """X with bin k multiplied by fac (an elementwise op on the device, no host upload)."""
+    X = X.clone()
+    X[..., k] *= fac
+    return X
 
 
 def resample(x, num, t=None, axis=0, window=None, domain="time"):
@@ -65,9 +74,7 @@ def resample(x, num, t=None, axis=0, window=None, domain="time"):
             X = X * _dev(Wf[:nX])
         X = X[..., :m2]
         if m % 2 == 0 and num != n:  # the unpaired bin at m/2
-            fac = np.ones(m2, dtype=np.float32)
-            fac[m // 2] = 2.0 if num < n else 0.5
-            X = X * _dev(fac)
+            X = _scale_bin(X, m // 2, 2.0 if num < n else 0.5)
         if W is not None and np.iscomplexobj(W):  # irfft reads DC (and Nyquist) as real
             X = X.clone()
             X[..., 0] = X[..., 0].real.to(torch.complex64)
@@ -85,9 +92,7 @@ def resample(x, num, t=None, axis=0, window=None, domain="time"):
         parts = []
         if num > n:  # upsampling: the unpaired bin is split into a pair
             if m % 2 == 0:
-                fac = np.ones(m2, dtype=np.float32)
-                fac[-1] = 0.5
-                first = first * _dev(fac)
+                first = _scale_bin(first, m2 - 1, 0.5)
                 parts = [first]
                 if num - m - 1:
                     parts.append(torch.zeros(X.shape[:-1] + (num - m - 1,),

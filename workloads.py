@@ -102,6 +102,18 @@ def _blue_stft(msig, k):
 
 
 #: name -> builder(msig, repeat) returning the calls to run
+def _hilbert(msig, k):
+    x = _randn(1 << 23, 9)
+    return [lambda: msig.hilbert(x)] * k
+
+
+def _tc_dft32(msig, k):
+    from mlx_signal_b200 import _kernels
+
+    z = torch.complex(_randn((1 << 18, 32), 10), _randn((1 << 18, 32), 11))
+    return [lambda: _kernels.dft32_tc(z)] * k
+
+
 WORKLOADS = {
     "welch_64x2p20_n1024": _welch,
     "welch_64x2p20_n256": _welch_n(256),
@@ -115,6 +127,8 @@ WORKLOADS = {
     "conv_8x2p22_t1025": _conv,
     "bluestein_welch_64x2p20_n1000": _blue_welch,
     "bluestein_stft_16x2p20_n1000": _blue_stft,
+    "hilbert_2p23": _hilbert,
+    "tc_dft32_2p18": _tc_dft32,
 }
 
 
