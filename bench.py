@@ -593,6 +593,7 @@ def secondary(x, steps, warmup, dist, clocks):
     out["general_shapes"] = general_shapes(x, dist, clocks, peak)
     out["batched_512_uneven"] = batched_uneven(dist, clocks, peak)
     out["rfft_1x2p23"] = large_rfft(dist, clocks, peak)
+    out["rfft_irfft_3x2p20"] = odd_factor_rfft(dist, clocks, peak)
     out["tc_dft32_stage"] = tc_dft32_stage(dist, clocks)
     out["fft_consumers"] = fft_consumers(dist, clocks, peak)
     out["reference_published_rows"] = published_rows(dist, clocks)
@@ -909,6 +910,7 @@ def large_rfft(dist, clocks, peak, log_n=23, seed=5):
     b = n * 4 + (n // 2 + 1) * 8
     if dist is not None:  # host-side checks and baselines at N = 1 only
         return {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak, "launches": 4}
+    ms_cufft = timed(lambda: torch.fft.rfft(x), 20, 3, dist, clocks)
     xh = x.cpu().numpy()
     ref = np.fft.rfft(xh.astype(np.float64))
     err = float(np.max(np.abs(X.cpu().numpy() - ref)) / np.max(np.abs(ref)))
@@ -920,9 +922,45 @@ def large_rfft(dist, clocks, peak, log_n=23, seed=5):
     cpu = b / statistics.median(t_cpu) / 1e9
     return {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
             "max_abs_err_rel_peak_vs_numpy_f64": err, "launches": 4,
+            "cufft_ms": ms_cufft, "speedup_vs_cufft": ms_cufft / ms,
             "cpu_baseline": {"GB/s": cpu, "cores": 1, "kind": "port",
                              "sample": "the full 2^23 transform, numpy.fft.rfft"},
             "speedup_vs_cpu": b / ms / 1e6 / cpu}
+
+
+def odd_factor_rfft(dist, clocks, peak, n=3 << 20, seed=6):
+    """Real transforms of a composite length (n = 3 2^20: three decimated branches of packed
+    2^19-point transforms around one radix-3 kernel on each side) through the public API,
+    against cuFFT (torch.fft) on the same device input and float64 numpy."""
+    import torch
+
+    from mlx_signal_b200 import fft as bfft
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    x = torch.randn(n, generator=g, device=dev)
+    X = bfft.rfft(x)
+    b = n * 4 + (n // 2 + 1) * 8
+    res = {}
+    for name, ours, lib in (("rfft", lambda: bfft.rfft(x), lambda: torch.fft.rfft(x)),
+                            ("irfft", lambda: bfft.irfft(X, n=n),
+                             lambda: torch.fft.irfft(X, n=n))):
+        ms = timed(ours, 20, 3, dist, clocks)
+        ms_lib = timed(lib, 20, 3, dist, clocks)
+        res[name] = {"ms": ms, "GB/s": b / ms / 1e6, "frac_hbm": b / ms / 1e6 / peak,
+                     "cufft_ms": ms_lib, "speedup_vs_cufft": ms_lib / ms}
+    if dist is None:
+        xh = x.cpu().numpy().astype(np.float64)
+        ref = np.fft.rfft(xh)
+        res["rfft"]["max_abs_err_rel_peak_vs_numpy_f64"] = float(
+            np.max(np.abs(X.cpu().numpy() - ref)) / np.max(np.abs(ref)))
+        back = bfft.irfft(X, n=n).cpu().numpy()
+        ref_b = np.fft.irfft(X.cpu().numpy().astype(np.complex128), n=n)
+        res["irfft"]["max_abs_err_rel_peak_vs_numpy_f64"] = float(
+            np.max(np.abs(back - ref_b)) / np.max(np.abs(ref_b)))
+    res["launches_per_call"] = 5
+    return res
 
 
 def summarize(sec: dict) -> dict:
@@ -957,7 +995,15 @@ def summarize(sec: dict) -> dict:
         bu = sec["batched_512_uneven"]
         ms["batch512"] = [r(bu["ms_batched"] * 1e3), r(bu["frac_hbm"]), r(bu["speedup_vs_plain"])]
     if "rfft_1x2p23" in sec:
-        ms["rfft_2p23"] = [r(sec["rfft_1x2p23"]["ms"] * 1e3), r(sec["rfft_1x2p23"]["frac_hbm"])]
+        rf = sec["rfft_1x2p23"]
+        ms["rfft_2p23"] = [r(rf["ms"] * 1e3), r(rf["frac_hbm"])]
+        if "cufft_ms" in rf:
+            ms["rfft_2p23"].append(r(rf["speedup_vs_cufft"]))
+    if "rfft_irfft_3x2p20" in sec:
+        mx = sec["rfft_irfft_3x2p20"]
+        for k in ("rfft", "irfft"):
+            ms[k + "_3x2p20"] = [r(mx[k]["ms"] * 1e3), r(mx[k]["frac_hbm"]),
+                                 r(mx[k]["speedup_vs_cufft"])]
     out["us_and_frac_hbm"] = ms
     if "tc_dft32_stage" in sec:
         tc = sec["tc_dft32_stage"]

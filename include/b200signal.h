@@ -278,7 +278,8 @@ SP_API int sp_istft_c64(const float* z, int64_t rows, int nseg, int64_t ld_row, 
                         int hop, float* out, void* stream);
 
 /* Workspace bytes for the long transforms below (two N-point complex intermediates + the device
- * error word; N = n for sp_fft_c64, n/2 for the real transforms). Negative = error status. */
+ * error word; N = n for sp_fft_c64, n/2 for the real transforms, where N may also be C 2^e with
+ * C odd <= 15). Negative = error status. */
 SP_API int64_t sp_fft_workspace_size(int64_t n, int batch);
 
 /*
@@ -291,17 +292,22 @@ SP_API int sp_fft_c64(const float* in, float* out, int batch, int64_t n, int inv
                       void* workspace, size_t workspace_bytes, void* stream);
 
 /*
- * Real-input FFT of `batch` contiguous rows of n float32 (n even, n/2 a power of two in
- * [2^12, 2^26]): X rows of n/2+1 complex64 bins with row stride ldx_out (complex elements).
- * Replaces _fourstep.rfft_large (_fourstep.py:213-231) with its untangle (:195-210).
+ * Real-input FFT of `batch` contiguous rows of n float32: X rows of n/2+1 complex64 bins with row
+ * stride ldx_out (complex elements). n = 2 C 2^e with C odd in [1, 15] and e in [12, 26]: C = 1
+ * is the packed power-of-two transform (three passes + untangle); C > 1 splits the rows into C
+ * decimated branches (one deinterleave kernel), runs their packed 2^e-point transforms as one
+ * batch, and untangles and combines them with one radix-C kernel. Replaces _fourstep.rfft_large
+ * (_fourstep.py:213-231) with its untangle (:195-210) and, for composite lengths, the divisor
+ * split of _fourstep._choose_split (:55-72) over MLX's mixed-radix FFT.
  */
 SP_API int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t ldx_out,
                        void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * Inverse real FFT: X rows (stride ldx complex, nbins valid bins, DC/Nyquist taken as real,
- * missing bins zero) -> batch contiguous rows of n float32 (n even, n/2 a power of two in
- * [2^12, 2^26]). Replaces _fourstep.irfft_large (_fourstep.py:372-408).
+ * missing bins zero) -> batch contiguous rows of n float32, n = 2 C 2^e as for sp_rfft_c64
+ * (C > 1: one radix-C fold + pretwist kernel, the C branch inverses as one batch, one interleave
+ * kernel). Replaces _fourstep.irfft_large (_fourstep.py:372-408).
  */
 SP_API int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, int64_t n,
                         void* workspace, size_t workspace_bytes, void* stream);
@@ -317,6 +323,32 @@ SP_API int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int ba
  */
 SP_API int sp_hilbert_c64(const float* x, float* out, int batch, int64_t n, void* workspace,
                           size_t workspace_bytes, void* stream);
+
+/*
+ * Fourier-method resampling of `batch` contiguous real rows from n to num samples
+ * (scipy.signal.resample for real input, no window, time domain): the min(n, num)/2 + 1 lowest
+ * bins of rfft_n(x), the unpaired bin m/2 of an even m = min(n, num) doubled when num < n or
+ * halved when num > n, scaled by num/n, inverse-transformed to num samples. n and num each
+ * 2 C 2^e as for sp_rfft_c64; x, y, workspace 16-byte aligned; workspace
+ * sp_resample_workspace_size(n, num, batch) bytes, its error word at
+ * sp_fft_error_word(workspace, max(n, num)/2, batch). One forward and one inverse transform with
+ * the bin selection and scaling folded into their untangle / pretwist kernels. Replaces the
+ * reference's resample (resampling.py:60-176: rfft, slice, bin fix-up, scale, irfft as separate
+ * array operations).
+ */
+SP_API int64_t sp_resample_workspace_size(int64_t n, int64_t num, int batch);
+SP_API int sp_resample_f32(const float* x, int batch, int64_t n, float* y, int64_t num,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Process-wide sticky error of the long transforms: SP_ERR_TIMEOUT once any of their bounded
+ * waits has run out since the last clear (the kernels store it in mapped pinned host memory as
+ * well as in the workspace word), else 0. clear != 0 resets it after reading. A plain host load:
+ * no CUDA call, no synchronisation (a timeout becomes visible once the failing CTA has stored
+ * it; synchronise the stream first to cover every transform issued). No counterpart in the
+ * reference (its waits are not bounded).
+ */
+SP_API int sp_fft_sticky_error(int clear);
 
 /* Byte offset of the int error word inside a long-transform workspace (0 = ok, SP_ERR_TIMEOUT if
  * a tile copy wait gave up); read it after synchronising the stream. */

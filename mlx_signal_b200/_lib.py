@@ -107,6 +107,9 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "sp_fft_c64": (c_i, [c_fp, c_fp, c_i, c_i64, c_i, c_p, c_sz, c_p]),
     "sp_rfft_c64": (c_i, [c_fp, c_fp, c_i, c_i64, c_i64, c_p, c_sz, c_p]),
     "sp_irfft_f32": (c_i, [c_fp, c_i64, c_i, c_fp, c_i, c_i64, c_p, c_sz, c_p]),
+    "sp_resample_workspace_size": (c_i64, [c_i64, c_i64, c_i]),
+    "sp_fft_sticky_error": (c_i, [c_i]),
+    "sp_resample_f32": (c_i, [c_fp, c_i, c_i64, c_fp, c_i64, c_p, c_sz, c_p]),
     "sp_fft_error_word": (c_i, [c_p, c_i64, c_i, ctypes.POINTER(c_i64)]),
     "sp_fft_set_wait_limit": (ctypes.c_uint32, [ctypes.c_uint32]),
     "sp_hilbert_c64": (c_i, [c_fp, c_fp, c_i, c_i64, c_p, c_sz, c_p]),

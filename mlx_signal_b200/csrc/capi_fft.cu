@@ -7,6 +7,7 @@
 
 #include "capi_common.h"
 #include "fft3_kernels.cuh"
+#include "fft_mixed.cuh"
 
 namespace b2s {
 namespace {
@@ -15,6 +16,26 @@ constexpr int kMinLogN = 12, kMaxLogN = 26;
 
 // poll limit of the per-tile copy waits (sp_fft_set_wait_limit)
 std::atomic<uint32_t> g_wait_polls{kMbarSpinLimit};
+
+// Process-wide sticky error word in mapped, portable pinned host memory: the passes store a
+// timeout there as well as in the workspace word, so a watchdog reads it with a plain load (no
+// copy, no event). Allocated on first use; null if the allocation fails (the workspace word
+// still reports).
+int* sticky_word() {
+  static int* host = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) ==
+        cudaSuccess) {
+      *static_cast<volatile int*>(p) = 0;
+      host = static_cast<int*>(p);
+    } else {
+      (void)cudaGetLastError();
+    }
+  });
+  return host;
+}
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -137,6 +158,7 @@ int fft3(const float2* in, float2* s1, float2* s2, float2* out, int batch, int e
   p.batch = batch;
   p.inverse = inverse;
   p.err = err;
+  p.sticky = sticky_word();  // unified addressing: the host pointer is the device pointer
   p.ntiles = 0;
   p.wait_polls = g_wait_polls.load(std::memory_order_relaxed);
   const int l3 = ilog2_exact(R3), l2 = ilog2_exact(R2), l1 = ilog2_exact(R1);
@@ -191,6 +213,122 @@ double2 untangle_step(int64_t m) {
 
 int64_t ws_need(int64_t n_complex, int batch) { return 2 * int64_t(batch) * n_complex * 8 + 256; }
 
+// Real length n = 2 C 2^e with C odd in [1, kMaxMixC] and e in [kMinLogN, kMaxLogN].
+int split_real(int64_t n, int* C, int* e, const char* who) {
+  int64_t h = n / 2, odd = h;
+  while (odd > 0 && odd % 2 == 0) odd /= 2;
+  const int le = (n > 0 && n % 2 == 0 && odd <= kMaxMixC) ? ilog2_exact(h / odd) : -1;
+  if (le < kMinLogN || le > kMaxLogN) {
+    set_error("%s: length %lld is not 2 C 2^e with C odd <= %d and e in [%d, %d]", who,
+              (long long)n, kMaxMixC, kMinLogN, kMaxLogN);
+    return SP_ERR_UNSUPPORTED;
+  }
+  *C = int(odd);
+  *e = le;
+  return SP_OK;
+}
+
+// W_n^m = exp(-i pi / C) for n = 2 C m, in FP64
+double2 half_branch_twiddle(int C) {
+  const double t = 3.141592653589793238462643383279502884 / double(C);
+  return make_double2(std::cos(t), -std::sin(t));
+}
+
+template <int C>
+cudaError_t launch_combine_t(unsigned grid, cudaStream_t s, const float2* Z, float2* X, int64_t m,
+                             int64_t ldx, int64_t nout) {
+  return launch_pdl(k_mixed_combine<C>, dim3(grid), kUntB, 0, s, Z, X, m, ldx, nout,
+                    half_branch_twiddle(C));
+}
+
+template <int C>
+cudaError_t launch_fold_t(unsigned grid, cudaStream_t s, const float2* X, int64_t ldx,
+                          int64_t nbins, float2* Yp, int64_t m, float scale, int64_t kfix,
+                          float ffix) {
+  return launch_pdl(k_mixed_fold_pretwist<C>, dim3(grid), kUntB, 0, s, X, ldx, nbins, Yp, m,
+                    half_branch_twiddle(C), scale, kfix, ffix);
+}
+
+#define B2S_MIXED_SWITCH(C, CALL)                                         \
+  switch (C) {                                                            \
+    case 3: return CALL(3);                                               \
+    case 5: return CALL(5);                                               \
+    case 7: return CALL(7);                                               \
+    case 9: return CALL(9);                                               \
+    case 11: return CALL(11);                                             \
+    case 13: return CALL(13);                                             \
+    case 15: return CALL(15);                                             \
+    default: return cudaErrorInvalidValue;                                \
+  }
+
+cudaError_t launch_combine(int C, unsigned grid, cudaStream_t s, const float2* Z, float2* X,
+                           int64_t m, int64_t ldx, int64_t nout) {
+#define B2S_CALL(c) launch_combine_t<c>(grid, s, Z, X, m, ldx, nout)
+  B2S_MIXED_SWITCH(C, B2S_CALL)
+#undef B2S_CALL
+}
+
+cudaError_t launch_fold(int C, unsigned grid, cudaStream_t s, const float2* X, int64_t ldx,
+                        int64_t nbins, float2* Yp, int64_t m, float scale, int64_t kfix,
+                        float ffix) {
+#define B2S_CALL(c) launch_fold_t<c>(grid, s, X, ldx, nbins, Yp, m, scale, kfix, ffix)
+  B2S_MIXED_SWITCH(C, B2S_CALL)
+#undef B2S_CALL
+}
+#undef B2S_MIXED_SWITCH
+
+// One-sided spectrum (bins below nout, row stride ldx) of `batch` real rows of n = 2 C m
+// samples; s1, s2 hold batch n/2 complex each and err follows them.
+int rfft_real(const float* x, float2* X, int batch, int C, int e, int64_t ldx, int64_t nout,
+              float2* s1, float2* s2, int* err, cudaStream_t s) {
+  const int64_t m = int64_t(1) << e;
+  int st;
+  if (C == 1) {
+    // the n real samples are m interleaved complex values; Z lands in s1 (free after pass 2)
+    if ((st = fft3(reinterpret_cast<const float2*>(x), s1, s2, s1, batch, e, 0, err, s)))
+      return st;
+    B2S_CHECK_CUDA(launch_pdl(k_rfft_untangle, dim3(untangle_blocks(m, batch)), kUntB, 0, s,
+                              static_cast<const float2*>(s1), X, m, ldx, nout, untangle_step(m)),
+                   "rfft untangle launch");
+    return SP_OK;
+  }
+  const int64_t M = 2 * m;
+  // branches D_s (batch C rows of M reals) in s2; their packed transforms Z_s land in s1
+  B2S_CHECK_CUDA(launch_pdl(k_mixed_deinterleave, dim3(unsigned(batch * (M / kMixQ))), kMixB, 0,
+                            s, x, reinterpret_cast<float*>(s2), C, M),
+                 "mixed deinterleave launch");
+  if ((st = fft3(s2, s1, s2, s1, batch * C, e, 0, err, s))) return st;
+  const unsigned grid = unsigned(cdiv(m / 2 + 1, kUntB) * batch);
+  B2S_CHECK_CUDA(launch_combine(C, grid, s, s1, X, m, ldx, nout), "mixed combine launch");
+  return SP_OK;
+}
+
+// Real rows (n = 2 C m samples each) from one-sided spectra X (nbins bins, row stride ldx),
+// every bin times scale and bin kfix also times ffix.
+int irfft_real(const float2* X, int64_t ldx, int64_t nbins, float* y, int batch, int C, int e,
+               float scale, int64_t kfix, float ffix, float2* s1, float2* s2, int* err,
+               cudaStream_t s) {
+  const int64_t m = int64_t(1) << e;
+  int st;
+  if (C == 1) {
+    B2S_CHECK_CUDA(launch_pdl(k_irfft_pretwist, dim3(untangle_blocks(m, batch)), kUntB, 0, s, X,
+                              ldx, nbins, s2, m, untangle_step(m), scale, kfix, ffix),
+                   "irfft pretwist launch");
+    // Y (in s2) -> S1 (s1) -> S2 (s2, Y already consumed by pass 1) -> y
+    return fft3(s2, s1, s2, reinterpret_cast<float2*>(y), batch, e, 1, err, s);
+  }
+  const int64_t M = 2 * m;
+  const unsigned grid = unsigned(cdiv(m / 2 + 1, kUntB) * batch);
+  B2S_CHECK_CUDA(launch_fold(C, grid, s, X, ldx, nbins, s2, m, scale, kfix, ffix),
+                 "mixed fold launch");
+  // packed branch spectra (s2) -> branch signals D_s in s1 -> interleaved into y
+  if ((st = fft3(s2, s1, s2, s1, batch * C, e, 1, err, s))) return st;
+  B2S_CHECK_CUDA(launch_pdl(k_mixed_interleave, dim3(unsigned(batch * (M / kMixQ))), kMixB, 0,
+                            s, reinterpret_cast<const float*>(s1), y, C, M),
+                 "mixed interleave launch");
+  return SP_OK;
+}
+
 }  // namespace
 }  // namespace b2s
 
@@ -203,7 +341,9 @@ int64_t sp_fft_workspace_size(int64_t n, int batch) {
     set_error("batch must be >= 1");
     return SP_ERR_ARG;
   }
-  const int st = check_n(n, &e);
+  int C;
+  const int st = check_n(n, &e) == SP_OK ? SP_OK : split_real(2 * n, &C, &e,
+                                                              "sp_fft_workspace_size");
   if (st != SP_OK) return st;
   return ws_need(n, batch);
 }
@@ -235,35 +375,25 @@ int sp_fft_c64(const float* in, float* out, int batch, int64_t n, int inverse, v
 int sp_rfft_c64(const float* x, float* X, int batch, int64_t n, int64_t ldx_out, void* workspace,
                 size_t workspace_bytes, void* stream) {
   using namespace b2s;
-  int e;
-  if (n % 2) {
-    set_error("sp_rfft_c64: n must be even");
-    return SP_ERR_UNSUPPORTED;
-  }
-  const int64_t m = n / 2;
-  int st = check_n(m, &e);
+  int e, C;
+  int st = split_real(n, &C, &e, "sp_rfft_c64");
   if (st != SP_OK) return st;
-  if (!x || !X || !workspace || batch < 1 || ldx_out < m + 1 || !aligned16(x) ||
+  const int64_t h = n / 2;
+  if (!x || !X || !workspace || batch < 1 || ldx_out < h + 1 || !aligned16(x) ||
       !aligned16(workspace) || (reinterpret_cast<uintptr_t>(X) & 7u)) {
     set_error("sp_rfft_c64: null or misaligned pointer, batch < 1 or ldx_out < n/2+1");
     return SP_ERR_ARG;
   }
-  if (int64_t(workspace_bytes) < ws_need(m, batch)) {
-    set_error("workspace too small: need %lld bytes", (long long)ws_need(m, batch));
+  if (int64_t(workspace_bytes) < ws_need(h, batch)) {
+    set_error("workspace too small: need %lld bytes", (long long)ws_need(h, batch));
     return SP_ERR_WORKSPACE;
   }
   auto s = static_cast<cudaStream_t>(stream);
   float2* s1 = static_cast<float2*>(workspace);
-  float2* s2 = s1 + int64_t(batch) * m;
-  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * m);
+  float2* s2 = s1 + int64_t(batch) * h;
+  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * h);
   B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
-  // the n real samples are m interleaved complex values; Z lands in s1 (free after pass 2)
-  if ((st = fft3(reinterpret_cast<const float2*>(x), s1, s2, s1, batch, e, 0, err, s))) return st;
-  B2S_CHECK_CUDA(launch_pdl(k_rfft_untangle, dim3(untangle_blocks(m, batch)), kUntB, 0, s,
-                            static_cast<const float2*>(s1), reinterpret_cast<float2*>(X), m,
-                            ldx_out, untangle_step(m)),
-                 "rfft untangle launch");
-  return SP_OK;
+  return rfft_real(x, reinterpret_cast<float2*>(X), batch, C, e, ldx_out, h + 1, s1, s2, err, s);
 }
 
 int sp_hilbert_c64(const float* x, float* out, int batch, int64_t n, void* workspace,
@@ -306,34 +436,84 @@ int sp_hilbert_c64(const float* x, float* out, int batch, int64_t n, void* works
 int sp_irfft_f32(const float* X, int64_t ldx, int nbins, float* x, int batch, int64_t n,
                  void* workspace, size_t workspace_bytes, void* stream) {
   using namespace b2s;
-  int e;
-  if (n % 2) {
-    set_error("sp_irfft_f32: n must be even");
-    return SP_ERR_UNSUPPORTED;
-  }
-  const int64_t m = n / 2;
-  int st = check_n(m, &e);
+  int e, C;
+  int st = split_real(n, &C, &e, "sp_irfft_f32");
   if (st != SP_OK) return st;
+  const int64_t h = n / 2;
   if (!X || !x || !workspace || batch < 1 || nbins < 1 || ldx < nbins || !aligned16(x) ||
       !aligned16(workspace) || (reinterpret_cast<uintptr_t>(X) & 7u)) {
     set_error("sp_irfft_f32: null or misaligned pointer or bad sizes");
     return SP_ERR_ARG;
   }
-  if (int64_t(workspace_bytes) < ws_need(m, batch)) {
-    set_error("workspace too small: need %lld bytes", (long long)ws_need(m, batch));
+  if (int64_t(workspace_bytes) < ws_need(h, batch)) {
+    set_error("workspace too small: need %lld bytes", (long long)ws_need(h, batch));
     return SP_ERR_WORKSPACE;
   }
   auto s = static_cast<cudaStream_t>(stream);
   float2* s1 = static_cast<float2*>(workspace);
-  float2* s2 = s1 + int64_t(batch) * m;
-  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * m);
+  float2* s2 = s1 + int64_t(batch) * h;
+  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * h);
   B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
-  B2S_CHECK_CUDA(launch_pdl(k_irfft_pretwist, dim3(untangle_blocks(m, batch)), kUntB, 0, s,
-                            reinterpret_cast<const float2*>(X), ldx, nbins, s2, m,
-                            untangle_step(m)),
-                 "irfft pretwist launch");
-  // Y (in s2) -> S1 (s1) -> S2 (s2, Y already consumed by pass 1) -> x
-  return fft3(s2, s1, s2, reinterpret_cast<float2*>(x), batch, e, 1, err, s);
+  return irfft_real(reinterpret_cast<const float2*>(X), ldx, nbins, x, batch, C, e, 1.0f, -1,
+                    1.0f, s1, s2, err, s);
+}
+
+int64_t sp_resample_workspace_size(int64_t n, int64_t num, int batch) {
+  using namespace b2s;
+  int e, C;
+  int st;
+  if (batch < 1) {
+    set_error("batch must be >= 1");
+    return SP_ERR_ARG;
+  }
+  if ((st = split_real(n, &C, &e, "sp_resample_f32")) ||
+      (st = split_real(num, &C, &e, "sp_resample_f32")))
+    return st;
+  const int64_t nc = (n > num ? n : num) / 2, m2 = (n < num ? n : num) / 2 + 1;
+  return ws_need(nc, batch) + cdiv(int64_t(batch) * m2 * 8, 256) * 256;
+}
+
+int sp_resample_f32(const float* x, int batch, int64_t n, float* y, int64_t num, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+  using namespace b2s;
+  int ef, Cf, ei, Ci;
+  int st;
+  if ((st = split_real(n, &Cf, &ef, "sp_resample_f32")) ||
+      (st = split_real(num, &Ci, &ei, "sp_resample_f32")))
+    return st;
+  if (!x || !y || !workspace || batch < 1 || !aligned16(x) || !aligned16(y) ||
+      !aligned16(workspace)) {
+    set_error("sp_resample_f32: null or misaligned (16 B) pointer, or batch < 1");
+    return SP_ERR_ARG;
+  }
+  const int64_t need = sp_resample_workspace_size(n, num, batch);
+  if (int64_t(workspace_bytes) < need) {
+    set_error("workspace too small: need %lld bytes", (long long)need);
+    return SP_ERR_WORKSPACE;
+  }
+  const int64_t nc = (n > num ? n : num) / 2, m = n < num ? n : num, m2 = m / 2 + 1;
+  auto s = static_cast<cudaStream_t>(stream);
+  float2* s1 = static_cast<float2*>(workspace);
+  float2* s2 = s1 + int64_t(batch) * nc;
+  int* err = reinterpret_cast<int*>(s2 + int64_t(batch) * nc);
+  float2* Xb = reinterpret_cast<float2*>(reinterpret_cast<char*>(err) + 256);
+  B2S_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error word reset");
+  // the m2 lowest bins of rfft_n(x); the unpaired bin m/2 of an even m is doubled (joining the
+  // +-m/2 pair, downsampling) or halved (split into a pair, upsampling); scale num/n
+  if ((st = rfft_real(x, Xb, batch, Cf, ef, m2, m2, s1, s2, err, s))) return st;
+  const int64_t kfix = (m % 2 == 0 && num != n) ? m / 2 : -1;
+  const float ffix = num < n ? 2.0f : 0.5f;
+  return irfft_real(Xb, m2, m2, y, batch, Ci, ei, float(double(num) / double(n)), kfix, ffix, s1,
+                    s2, err, s);
+}
+
+int sp_fft_sticky_error(int clear) {
+  int* w = b2s::sticky_word();
+  if (!w) return 0;
+  volatile int* v = w;
+  const int st = *v;
+  if (clear && st) *v = 0;
+  return st;
 }
 
 uint32_t sp_fft_set_wait_limit(uint32_t polls) {

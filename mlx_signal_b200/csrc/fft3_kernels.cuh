@@ -21,9 +21,10 @@
 //    per element in FP32) -- no twiddle table in global memory;
 //  * the inverse transform is conj(FFT(conj(x))) / N with 1/N folded into pass 1.
 // Every mbarrier wait is bounded; on timeout the CTA records SP_ERR_TIMEOUT in the error word,
-// waits (bounded) for its own copies and returns without touching the data. The limit of the
-// wait for each tile is a launch parameter (sp_fft_set_wait_limit), so a host watchdog test can
-// make it run out.
+// waits (bounded) for its own copies and returns without touching the data; the code is also
+// stored in a process-wide word in mapped pinned host memory (sp_fft_sticky_error). The limit of
+// the wait for each tile is a launch parameter (sp_fft_set_wait_limit), so a host watchdog test
+// can make it run out.
 #pragma once
 
 #include <cuda.h>
@@ -43,6 +44,8 @@ struct Fft3Params {
   int batch;
   int inverse;         // 1: conj on load (pass 1) and on store (pass 3), scale 1/N in pass 1
   int* err;            // device error word (0 = ok)
+  int* sticky;         // process-wide word in mapped pinned host memory (or null): a timeout
+                       // also lands here, so a host watchdog reads it without a copy
   int ntiles;          // tiles of this pass (a persistent CTA walks tile, tile + gridDim.x, ...)
   uint32_t wait_polls; // poll limit of the wait for each tile's copy (kMbarSpinLimit by default)
 };
@@ -261,6 +264,10 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
     if (!ok) {
       if (threadIdx.x == 0) {
         atomicExch(pr.err, SP_ERR_TIMEOUT);
+        if (pr.sticky) {
+          *reinterpret_cast<volatile int*>(pr.sticky) = SP_ERR_TIMEOUT;
+          __threadfence_system();
+        }
         // bounded second waits (full limit) for the copies still in flight, so that no TMA
         // write lands in this CTA's shared memory after it exits
         (void)mbar_wait(bar + j, par);
@@ -339,10 +346,11 @@ constexpr int kUntT = 8;    // indices per thread
 
 // Packed real FFT untangle (n = 2m real samples viewed as m complex z, Z = FFT_m(z)):
 //   X_k = (Z_k + conj Z_{m-k})/2 - i w_k (Z_k - conj Z_{m-k})/2, w_k = exp(-i pi k/m), k < m;
-//   X_m = Re Z_0 - Im Z_0. Index k in [0, m/2] produces X_k and X_{m-k}.
+//   X_m = Re Z_0 - Im Z_0. Index k in [0, m/2] produces X_k and X_{m-k}; only bins below nout
+//   are written (nout = m + 1 for the whole one-sided spectrum).
 __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restrict__ Z,
                                                          float2* __restrict__ X, int64_t m,
-                                                         int64_t ldx, double2 d) {
+                                                         int64_t ldx, int64_t nout, double2 d) {
   fft_pdl_wait();
   fft_pdl_trigger();
   const int64_t half = m / 2 + 1;
@@ -370,7 +378,7 @@ __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restric
       if (k == 0) {
         const float2 z0 = zks[j];
         x[0] = make_float2(z0.x + z0.y, 0.f);
-        x[m] = make_float2(z0.x - z0.y, 0.f);
+        if (m < nout) x[m] = make_float2(z0.x - z0.y, 0.f);
       } else {
         const float2 zk = zks[j], zm = zms[j];
         const float2 wf = make_float2(float(w.x), float(w.y));
@@ -378,8 +386,8 @@ __global__ void __launch_bounds__(kUntB) k_rfft_untangle(const float2* __restric
         const float2 ze = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         const float2 zo = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y + zm.y));
         const float2 wz = cmul(wf, zo);
-        x[k] = make_float2(ze.x + wz.y, ze.y - wz.x);
-        if (2 * k != m) {
+        if (k < nout) x[k] = make_float2(ze.x + wz.y, ze.y - wz.x);
+        if (2 * k != m && m - k < nout) {
           const float2 wz2 = make_float2(wz.x, -wz.y);  // w' zo' = conj(w zo)
           x[m - k] = make_float2(ze.x + wz2.y, -ze.y - wz2.x);
         }
@@ -445,11 +453,13 @@ __global__ void __launch_bounds__(kUntB) k_hilbert_spectrum(const float2* __rest
 
 // Inverse of the untangle (irfft pre-twist): from X_0..X_m build the packed spectrum
 //   Y_k = E_k + i conj(w_k) O_k, E = (X_k + conj X_{m-k})/2, O = (X_k - conj X_{m-k})/2,
-// with X_0, X_m taken as real; then z = IFFT_m(Y) interleaves the n real samples.
+// with X_0, X_m taken as real; then z = IFFT_m(Y) interleaves the n real samples. Every bin is
+// multiplied by `scale`, and bin kfix (if any) also by ffix (the resample's unpaired bin).
 __global__ void __launch_bounds__(kUntB) k_irfft_pretwist(const float2* __restrict__ X,
-                                                          int64_t ldx, int nbins,
+                                                          int64_t ldx, int64_t nbins,
                                                           float2* __restrict__ Y, int64_t m,
-                                                          double2 d) {
+                                                          double2 d, float scale, int64_t kfix,
+                                                          float ffix) {
   fft_pdl_wait();
   fft_pdl_trigger();
   const int64_t half = m / 2 + 1;
@@ -462,7 +472,8 @@ __global__ void __launch_bounds__(kUntB) k_irfft_pretwist(const float2* __restri
     if (j >= nbins) return make_float2(0.f, 0.f);
     float2 v = x[j];
     if (j == 0 || j == m) v.y = 0.f;
-    return v;
+    const float f = j == kfix ? scale * ffix : scale;
+    return make_float2(v.x * f, v.y * f);
   };
   float2 xks[kUntT], xms[kUntT];  // every read first, as in the untangle
 #pragma unroll

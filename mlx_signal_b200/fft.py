@@ -5,8 +5,10 @@ _fft_core.py:55-104 -> _fourstep.rfft_large / irfft_large / fft_large / ifft_lar
 _fourstep.py:177-231, 372-408 -> _fourstep_metal.fft3_last for 2^21..2^26). Transforms whose
 complex length (n for fft/ifft, n/2 for rfft/irfft) is a power of two in
 [2^KERNEL_MIN_LOG2, 2^26] run the three-pass TMA-staged kernels (the C-ABI takes every power of
-two from 2^12); other lengths run cuFFT through torch.fft (the composed GPU path; the reference
-uses MLX's own FFT there). The default threshold 2^20 is where the kernels match cuFFT (measured:
+two from 2^12). Real transforms also take n = 2 C 2^e with C odd <= 15: the C decimated branches
+run as one batch of packed power-of-two transforms around one radix-C kernel on each side. Other
+lengths run cuFFT through torch.fft (the composed GPU path; the reference uses MLX's own FFT
+there). The default threshold 2^20 is where the kernels match cuFFT (measured:
 rfft 2^23 68 vs 66 us, 2^24 120 vs 132 us, 8 x 2^23 408 vs 459 us; shorter or batched-short
 transforms are faster in cuFFT). numpy.fft semantics for `n` (zero-pad or truncate) and `axis`.
 """
@@ -27,10 +29,38 @@ MIN_LOG2, MAX_LOG2 = 12, 26   # lengths the C-ABI accepts
 KERNEL_MIN_LOG2 = 20          # lengths the Python API routes to the kernels
 
 
+MAX_ODD = 15                  # largest odd factor C of a real length n = 2 C 2^e
+
+
 def _pow2_in_range(m: int) -> bool:
     """True when a complex transform of length m runs on the three-pass kernels."""
     lo = max(MIN_LOG2, KERNEL_MIN_LOG2)
     return m >= 1 and (m & (m - 1)) == 0 and lo <= m.bit_length() - 1 <= MAX_LOG2
+
+
+def _real_split(n: int) -> tuple[int, int] | None:
+    """(C, e) with n = 2 C 2^e, C odd <= MAX_ODD and e in the C-ABI's range, else None."""
+    if n < 2 or n % 2:
+        return None
+    h = n // 2
+    c = h
+    while c % 2 == 0:
+        c //= 2
+    e = (h // c).bit_length() - 1
+    if c > MAX_ODD or not MIN_LOG2 <= e <= MAX_LOG2:
+        return None
+    return c, e
+
+
+def _real_in_range(n: int) -> bool:
+    """True when a real transform of length n runs on the kernels: n/2 a power of two in the
+    three-pass range, or C 2^e (C odd <= 15; the C branches run as one batch of packed 2^e-point
+    transforms) with n/2 >= 2^KERNEL_MIN_LOG2."""
+    sp = _real_split(n)
+    if sp is None:
+        return False
+    c, _ = sp
+    return _pow2_in_range(n // 2) if c == 1 else n // 2 >= (1 << KERNEL_MIN_LOG2)
 
 
 def _notice_long(func_name: str, m: int) -> None:
@@ -59,6 +89,13 @@ def _fit(t: torch.Tensor, n: int) -> torch.Tensor:
     return torch.cat([t, pad], dim=-1)
 
 
+def _rows16(t: torch.Tensor, rows: int, n: int) -> torch.Tensor:
+    """t as a contiguous (rows, n) tensor whose data starts on a 16-byte boundary (the TMA
+    tensor maps' base rule; a view into the middle of a buffer is copied)."""
+    r = t.reshape(rows, n).contiguous()
+    return r if r.data_ptr() % 16 == 0 else r.clone()
+
+
 def _workspace(n_complex: int, batch: int, dev) -> torch.Tensor:
     nbytes = _lib.load().sp_fft_workspace_size(n_complex, batch)
     if nbytes < 0:
@@ -72,55 +109,28 @@ class DeviceWaitTimeout(_lib.KernelError):
 
 
 class _StatusWatch:
-    """Host watchdog for the long transforms' device error words. After each launch the word is
-    copied (stream-ordered, no synchronisation) into a slot of a pinned ring with an event; a
-    later call, or `device_status()`, reads the slots whose events completed and raises
-    DeviceWaitTimeout for a non-zero word."""
-
-    SLOTS = 64
+    """Host watchdog for the long transforms' bounded device waits. A wait that runs out stores
+    SP_ERR_TIMEOUT in the transform's workspace word and in a process-wide sticky word in mapped
+    pinned host memory (sp_fft_sticky_error); a later call, or `device_status()`, reads the
+    sticky word with a plain host load (no copy, no event, allowed while a CUDA graph is being
+    captured) and raises DeviceWaitTimeout. `record` only notes which kind of transform ran
+    last, for the message."""
 
     def __init__(self):
-        self.host = None
-        self.live: list = []  # (slot, event, what)
-        self.next = 0
+        self.last = "long transform"
 
     def record(self, ws: torch.Tensor, n_complex: int, batch: int, what: str) -> None:
-        if self.host is None:
-            self.host = torch.zeros(self.SLOTS, dtype=torch.int32, pin_memory=True)
-        import ctypes
+        self.last = what
 
-        off = ctypes.c_int64(0)
-        _lib.check(_lib.load().sp_fft_error_word(ws.data_ptr(), n_complex, batch,
-                                                 ctypes.byref(off)), "sp_fft_error_word")
-        if len(self.live) >= self.SLOTS:  # ring full: the oldest slot must be read first
-            self.poll(wait_oldest=True)
-        slot = self.next
-        self.next = (self.next + 1) % self.SLOTS
-        word = ws[off.value : off.value + 4].view(torch.int32)
-        self.host[slot : slot + 1].copy_(word, non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record()
-        self.live.append((slot, ev, what))
-
-    def poll(self, wait_oldest: bool = False, wait_all: bool = False) -> int:
-        status = 0
-        keep = []
-        for i, (slot, ev, what) in enumerate(self.live):
-            if wait_all or (wait_oldest and i == 0):
-                ev.synchronize()
-            if not ev.query():
-                keep.append((slot, ev, what))
-                continue
-            word = int(self.host[slot])
-            if word != 0 and status == 0:
-                status = word
-                failed = what
-        self.live = keep
+    def poll(self, wait_all: bool = False) -> int:
+        if wait_all and torch.cuda.is_available() and not torch.cuda.is_current_stream_capturing():
+            torch.cuda.synchronize()
+        status = int(_lib.load().sp_fft_sticky_error(1))
         if status != 0:
             text = ("a bounded device wait ran out; the output of that transform is undefined"
                     if status == _lib.SP_ERR_TIMEOUT else "device error word set")
-            raise DeviceWaitTimeout(failed, status, text)
-        return status
+            raise DeviceWaitTimeout(self.last, status, text)
+        return 0
 
 
 _watch = _StatusWatch()
@@ -141,10 +151,10 @@ def rfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
     x = _last(x, axis)
     n = x.shape[-1] if n is None else int(n)
     x = _fit(x, n)
-    if n % 2 == 0 and _pow2_in_range(n // 2):
+    if _real_in_range(n):
         batch = tuple(x.shape[:-1])
         rows = math.prod(batch)
-        xr = x.reshape(rows, n).contiguous()
+        xr = _rows16(x, rows, n)
         out = torch.empty((rows, n // 2 + 1), dtype=torch.complex64, device=x.device)
         ws = _workspace(n // 2, rows, x.device)
         _lib.check(_lib.load().sp_rfft_c64(xr.data_ptr(), out.data_ptr(), rows, n, n // 2 + 1,
@@ -164,7 +174,7 @@ def irfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
         X = X.to(torch.complex64)
     X = _last(X, axis)
     n = 2 * (X.shape[-1] - 1) if n is None else int(n)
-    if n % 2 == 0 and _pow2_in_range(n // 2):
+    if _real_in_range(n):
         batch = tuple(X.shape[:-1])
         rows = math.prod(batch)
         nb = min(X.shape[-1], n // 2 + 1)
@@ -191,7 +201,7 @@ def _cfft(a, n, axis, inverse: bool) -> torch.Tensor:
     if _pow2_in_range(n):
         batch = tuple(z.shape[:-1])
         rows = math.prod(batch)
-        zr = z.reshape(rows, n).contiguous()
+        zr = _rows16(z, rows, n)
         out = torch.empty((rows, n), dtype=torch.complex64, device=z.device)
         ws = _workspace(n, rows, z.device)
         _lib.check(_lib.load().sp_fft_c64(zr.data_ptr(), out.data_ptr(), rows, n, int(inverse),

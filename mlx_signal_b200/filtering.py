@@ -56,7 +56,7 @@ def _fused(x: torch.Tensor, N: int) -> torch.Tensor:
     """Analytic signal of the rows of x (..., N) float32 through sp_hilbert_c64."""
     batch = tuple(x.shape[:-1])
     rows = math.prod(batch)
-    xr = x.reshape(rows, N).contiguous()
+    xr = _fft._rows16(x, rows, N)
     out = torch.empty((rows, N), dtype=torch.complex64, device=x.device)
     ws = _fft._workspace(N, rows, x.device)
     _lib.check(_lib.load().sp_hilbert_c64(xr.data_ptr(), out.data_ptr(), rows, N, ws.data_ptr(),

@@ -6,15 +6,21 @@ fftshift order; a real input's one-sided spectrum takes the window folded onto i
 m = min(num, n) lowest-frequency bins, split (upsampling) or join (downsampling) the unpaired
 bin at m/2 when m is even, scale by num / n and inverse-transform to num samples. Transforms run
 on the three-pass kernels where `mlx_signal_b200.fft` covers their length, cuFFT otherwise.
+A real time-domain input without a window, whose lengths n and num both run on the kernels, takes
+one C-ABI call (`sp_resample_f32`): the forward transform writes only the kept bins, and the bin
+fix-up and the num/n scale are folded into the inverse transform's pretwist.
 """
 
 from __future__ import annotations
 
+import math
+
 import numpy as np
 import torch
 
+from . import _lib
 from . import fft as _fft
-from ._array import device, to_device, to_numpy
+from ._array import device, stream_handle, to_device, to_numpy
 from .windows import _window_np, device_vector
 
 __all__ = ["resample"]
@@ -50,6 +56,24 @@ def _scale_bin(X: torch.Tensor, k: int, fac: float) -> torch.Tensor:
     return X
 
 
+def _resample_fused(xa: torch.Tensor, num: int) -> torch.Tensor:
+    """Real rows (..., n) -> (..., num) through sp_resample_f32."""
+    n = xa.shape[-1]
+    batch = tuple(xa.shape[:-1])
+    rows = math.prod(batch)
+    xr = _fft._rows16(xa.to(torch.float32), rows, n)
+    out = torch.empty((rows, num), dtype=torch.float32, device=xa.device)
+    lib = _lib.load()
+    nbytes = int(lib.sp_resample_workspace_size(n, num, rows))
+    if nbytes < 0:
+        _lib.check(nbytes, "sp_resample_workspace_size")
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=xa.device)
+    _lib.check(lib.sp_resample_f32(xr.data_ptr(), rows, n, out.data_ptr(), num, ws.data_ptr(),
+                                   ws.numel(), stream_handle()), "sp_resample_f32")
+    _fft._watch.record(ws, max(n, num) // 2, rows, "resample")
+    return out.reshape(batch + (num,))
+
+
 def resample(x, num, t=None, axis=0, window=None, domain="time"):
     """Resample x to num samples along `axis` with the Fourier method. Returns the resampled
     signal, or (resampled, new_t) when sample positions t are given."""
@@ -64,7 +88,11 @@ def resample(x, num, t=None, axis=0, window=None, domain="time"):
     m = min(num, n)
     m2 = m // 2 + 1
     W = None if window is None else _freq_window(window, n)
-    if domain == "time" and not xa.is_complex():
+    if (domain == "time" and not xa.is_complex() and W is None and n > 0
+            and _fft._real_in_range(n) and _fft._real_in_range(num)):
+        _fft._watch.poll()
+        y = _resample_fused(xa, num)
+    elif domain == "time" and not xa.is_complex():
         X = _fft.rfft(xa, axis=-1)
         nX = X.shape[-1]
         if W is not None:

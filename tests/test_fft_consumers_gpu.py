@@ -180,3 +180,37 @@ def test_conv_ols_capi_windows(rng):
         o = out.cpu().numpy()
         assert peak_err(torch.from_numpy(o[:, :nout]), full[:, j0 : j0 + nout]) < 2e-6
         assert np.all(o[:, nout:] == 7.0)
+
+
+@pytest.mark.parametrize("n,num", [(1 << 14, 3 << 13), (3 << 13, 1 << 14), (5 << 13, 3 << 13),
+                                   (3 << 13, 5 << 13), (1 << 15, 1 << 14), (1 << 14, 1 << 15),
+                                   (3 << 13, 3 << 13), (15 << 13, 1 << 13)])
+def test_resample_fused_matches_scipy(rng, monkeypatch, n, num):
+    """Real input, no window: one sp_resample_f32 call (forward transform writing only the kept
+    bins, unpaired-bin fix-up and num/n scale inside the inverse pretwist), power-of-two and
+    odd-factor lengths, against float64 scipy."""
+    from mlx_signal_b200 import fft as bfft
+
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
+    assert bfft._real_in_range(n) and bfft._real_in_range(num)
+    x = rng.standard_normal((2, n)).astype(np.float32)
+    ref = sps.resample(x.astype(np.float64), num, axis=-1)
+    got = msig.resample(x, num, axis=-1)
+    assert tuple(got.shape) == ref.shape
+    assert peak_err(got, ref) < 5e-6
+    xt = np.ascontiguousarray(x.T)
+    got0 = msig.resample(xt, num, axis=0)
+    assert peak_err(got0, sps.resample(xt.astype(np.float64), num, axis=0)) < 5e-6
+    assert bfft.device_status() == 0
+
+
+def test_resample_fused_full_size(rng):
+    """2^22 -> 3 2^20 samples through the default routing (both lengths on the kernels), with
+    sample positions, against float64 scipy."""
+    n, num = 1 << 22, 3 << 20
+    x = rng.standard_normal(n).astype(np.float32)
+    t = np.arange(n) * 1e-3
+    got, nt = msig.resample(x, num, t=t)
+    ref, nt_ref = sps.resample(x.astype(np.float64), num, t=t)
+    assert peak_err(got, ref) < 5e-6
+    np.testing.assert_allclose(nt.cpu().numpy(), nt_ref, rtol=1e-6)

@@ -126,13 +126,19 @@ def test_bounded_wait_runs_out_and_reports_timeout(rng, monkeypatch):
     off = ctypes.c_int64(0)
     assert lib.sp_fft_error_word(ws.data_ptr(), n, 1, ctypes.byref(off)) == 0
     stream = torch.cuda.current_stream().cuda_stream
+    assert bfft.device_status() == 0 and lib.sp_fft_sticky_error(0) == 0
     prev = lib.sp_fft_set_wait_limit(0)
     try:
         assert lib.sp_fft_c64(x.data_ptr(), out.data_ptr(), 1, n, 0, ws.data_ptr(), ws.numel(),
                               stream) == 0
         torch.cuda.synchronize()
         assert int(ws[off.value : off.value + 4].view(torch.int32).item()) == _lib.SP_ERR_TIMEOUT
-        # the Python path: the watchdog raises on the host once the transform has completed
+        # the process-wide sticky word (mapped pinned host memory) holds it too until cleared
+        assert lib.sp_fft_sticky_error(0) == _lib.SP_ERR_TIMEOUT
+        with pytest.raises(bfft.DeviceWaitTimeout):
+            bfft.device_status()
+        assert lib.sp_fft_sticky_error(0) == 0
+        # the Python path: the watchdog raises on the host once the transform has run
         monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
         xr = torch.from_numpy(rng.standard_normal(2 * n).astype(np.float32)).cuda()
         bfft.rfft(xr)
@@ -160,3 +166,74 @@ def test_default_routing_uses_cufft_below_2p20(rng, monkeypatch):
     assert not bfft._pow2_in_range(1 << 19) and bfft._pow2_in_range(1 << 20)
     x = rng.standard_normal(1 << 14).astype(np.float32)
     assert _rel(bfft.rfft(x), np.fft.rfft(x.astype(np.float64))) < 5e-6
+
+
+@pytest.mark.parametrize("c", [3, 5, 7, 9, 11, 13, 15])
+def test_rfft_irfft_odd_factor_lengths(rng, c):
+    """n = 2 C 2^12: C decimated branches through one batch of packed 2^12-point transforms and
+    the radix-C untangle/combine and fold/pretwist kernels, against float64 numpy."""
+    n = 2 * c * (1 << 12)
+    assert bfft._real_split(n) == (c, 12) and bfft._real_in_range(n)
+    x = rng.standard_normal((2, n)).astype(np.float32)
+    ref = np.fft.rfft(x.astype(np.float64), axis=-1)
+    got = bfft.rfft(x)
+    assert tuple(got.shape) == ref.shape
+    for i in range(2):
+        assert _rel(got[i], ref[i]) < 5e-6
+    X = (rng.standard_normal((2, n // 2 + 1)) + 1j * rng.standard_normal((2, n // 2 + 1)))
+    X = X.astype(np.complex64)
+    back = bfft.irfft(X, n=n)
+    ref_back = np.fft.irfft(X.astype(np.complex128), n=n, axis=-1)
+    for i in range(2):
+        assert _rel(back[i], ref_back[i]) < 5e-6
+    assert bfft.device_status() == 0
+
+
+@pytest.mark.parametrize("n,nbins", [(3 << 13, 1000), (3 << 13, (3 << 12) + 1),
+                                     (5 << 13, (5 << 12) + 700), (15 << 13, 7)])
+def test_irfft_odd_factor_truncation_and_padding(rng, n, nbins):
+    """numpy irfft semantics on the mixed path: fewer bins than n/2+1 are zero-padded, more are
+    cut; the imaginary parts of DC and Nyquist are ignored."""
+    X = (rng.standard_normal(nbins) + 1j * rng.standard_normal(nbins)).astype(np.complex64)
+    assert _rel(bfft.irfft(X, n=n), np.fft.irfft(X.astype(np.complex128), n=n)) < 5e-6
+
+
+def test_odd_factor_structured_and_roundtrip(rng):
+    """A tone on a non-bin frequency and an impulse (exercise every residue class of the
+    combine), the largest packed size class here, and the irfft(rfft(x)) round trip."""
+    n = 3 << 20
+    t = np.arange(n)
+    tone = np.cos(2 * np.pi * (123456.25 / n) * t).astype(np.float32)
+    imp = np.zeros(n, np.float32)
+    imp[98765] = 1.0
+    for x in (tone, imp):
+        assert _rel(bfft.rfft(x), np.fft.rfft(x.astype(np.float64))) < 5e-6
+    x = rng.standard_normal((3, 7 << 13)).astype(np.float32)
+    assert _rel(bfft.irfft(bfft.rfft(x), n=7 << 13), x) < 5e-6
+    xt = np.ascontiguousarray(x.T)
+    assert _rel(bfft.rfft(xt, axis=0), np.fft.rfft(xt.astype(np.float64), axis=0)) < 5e-6
+
+
+def test_odd_factor_default_routing(monkeypatch):
+    """With the public threshold (2^20 complex points) a composite real length runs the kernels
+    once n/2 reaches 2^20; odd factors above 15 or packed lengths outside [2^12, 2^26] do not."""
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 20)
+    assert bfft._real_in_range(3 << 20) and not bfft._real_in_range(3 << 19)
+    assert bfft._real_split(17 << 14) is None and bfft._real_split(3 << 12) is None
+
+
+def test_long_transforms_capture_in_a_cuda_graph(rng):
+    """The public long transforms can be captured and replayed (the watchdog stands aside while
+    the stream captures): rfft of a power-of-two and of an odd-factor length, and irfft."""
+    from mlx_signal_b200 import graphs
+
+    for n in (1 << 14, 3 << 13):
+        x0 = torch.from_numpy(rng.standard_normal((2, n)).astype(np.float32)).cuda()
+        call = graphs.GraphedCall(lambda t: bfft.irfft(bfft.rfft(t) * 2.0, n=n), x0)
+        for _ in range(2):
+            x = rng.standard_normal((2, n)).astype(np.float32)
+            got = call(torch.from_numpy(x).cuda())
+            torch.cuda.synchronize()
+            assert _rel(got, 2.0 * x.astype(np.float64)) < 5e-6
+        del call
+    assert bfft.device_status() == 0

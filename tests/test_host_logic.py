@@ -144,3 +144,20 @@ def test_profiling_workloads_listed():
 
     assert workloads.main(["--list"]) == 0
     assert {"welch_64x2p20_n1024", "conv_8x2p22_t1025", "rfft_2p23"} <= set(workloads.WORKLOADS)
+
+
+def test_real_length_split_and_routing(monkeypatch):
+    """Real transform lengths n = 2 C 2^e (C odd <= 15, e in [12, 26]) and their routing
+    threshold; everything else goes to the composed path."""
+    from mlx_signal_b200 import fft as bfft
+
+    assert bfft._real_split(1 << 23) == (1, 22)
+    assert bfft._real_split(3 << 20) == (3, 19)
+    assert bfft._real_split(15 << 13) == (15, 12)
+    for n in (0, 1, 3 << 11, 17 << 14, 600_000, (1 << 27) + 2, 1 << 28, 9999):
+        assert bfft._real_split(n) is None
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 20)
+    assert bfft._real_in_range(1 << 21) and not bfft._real_in_range(1 << 20)
+    assert bfft._real_in_range(3 << 20) and not bfft._real_in_range(3 << 19)
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
+    assert bfft._real_in_range(3 << 13) and bfft._real_in_range(1 << 13)

@@ -101,7 +101,17 @@ def _blue_stft(msig, k):
     return [lambda: msig.stft(x, nperseg=1000)] * k
 
 
-#: name -> builder(msig, repeat) returning the calls to run
+def _rfft_odd(msig, k):
+    x = _randn(3 << 20, 12)
+    X = msig.fft.rfft(x)
+    return [lambda: msig.fft.rfft(x), lambda: msig.fft.irfft(X, n=3 << 20)] * k
+
+
+def _resample_odd(msig, k):
+    x = _randn(1 << 22, 13)
+    return [lambda: msig.resample(x, 3 << 20)] * k
+
+
 def _hilbert(msig, k):
     x = _randn(1 << 23, 9)
     return [lambda: msig.hilbert(x)] * k
@@ -129,6 +139,8 @@ WORKLOADS = {
     "bluestein_stft_16x2p20_n1000": _blue_stft,
     "hilbert_2p23": _hilbert,
     "tc_dft32_2p18": _tc_dft32,
+    "rfft_irfft_3x2p20": _rfft_odd,
+    "resample_2p22_to_3x2p20": _resample_odd,
 }
 
 
