@@ -1,16 +1,22 @@
-"""Long power-of-two FFTs on B200: rfft / irfft / fft / ifft along one axis.
+"""Long FFTs on B200: rfft / irfft / fft / ifft along one axis.
 
 Counterpart of the reference's FFT routing for long transforms (src/mlx_signal_processing/
 _fft_core.py:55-104 -> _fourstep.rfft_large / irfft_large / fft_large / ifft_large,
-_fourstep.py:177-231, 372-408 -> _fourstep_metal.fft3_last for 2^21..2^26). Transforms whose
-complex length (n for fft/ifft, n/2 for rfft/irfft) is a power of two in
-[2^KERNEL_MIN_LOG2, 2^26] run the three-pass TMA-staged kernels (the C-ABI takes every power of
-two from 2^12). Real transforms also take n = 2 C 2^e with C odd <= 15: the C decimated branches
-run as one batch of packed power-of-two transforms around one radix-C kernel on each side. Other
-lengths run cuFFT through torch.fft (the composed GPU path; the reference uses MLX's own FFT
-there). The default threshold 2^20 is where the kernels match cuFFT (measured:
-rfft 2^23 68 vs 66 us, 2^24 120 vs 132 us, 8 x 2^23 408 vs 459 us; shorter or batched-short
-transforms are faster in cuFFT). numpy.fft semantics for `n` (zero-pad or truncate) and `axis`.
+_fourstep.py:177-231, 372-408 -> _fourstep_metal.fft3_last for 2^21..2^26). The C-ABI takes
+complex lengths that are powers of two in [2^12, 2^26] (three TMA-staged passes) and real
+lengths n = 2 C 2^e with C odd <= 15 (the C decimated branches as one batch of packed
+power-of-two transforms around one radix-C kernel on each side). This module routes a transform
+to those kernels where they are faster than cuFFT (torch.fft) on B200, by device time measured
+with CUDA-graph replay (microseconds, ours / cuFFT):
+  complex fft  2^21: 29.9 / 20.1   2^22: 47.2 / 48.8   2^23: 82.1 / 97.9   2^24: 156 / 185
+  rfft         n = 2^22: 34.9 / 25.7   2^23: 56.4 / 59.2   2^25: 203 / 231
+  irfft        n = 2^22: 42.9 / 40.3   2^23: 72.1 / 88.8   2^25: 244 / 356
+  irfft        n = 3 2^22: 117 / 145   5 2^22: 191 / 230   (3 2^20: 42.7 / 41.1)
+  rfft         n = 3 2^22: 124 / 99.6  (odd-factor forward: cuFFT is faster at every size)
+i.e. from 2^KERNEL_MIN_LOG2 = 2^22 complex points (n/2 for the real transforms); odd-factor
+forward transforms stay on cuFFT unless ODD_FORWARD is set (the fused resample uses them
+directly). Other lengths run cuFFT (the composed GPU path; the reference uses MLX's own FFT
+there). numpy.fft semantics for `n` (zero-pad or truncate) and `axis`.
 """
 
 from __future__ import annotations
@@ -26,7 +32,9 @@ from ._config import composed_path_notice
 __all__ = ["DeviceWaitTimeout", "device_status", "fft", "ifft", "irfft", "rfft"]
 
 MIN_LOG2, MAX_LOG2 = 12, 26   # lengths the C-ABI accepts
-KERNEL_MIN_LOG2 = 20          # lengths the Python API routes to the kernels
+KERNEL_MIN_LOG2 = 22          # lengths the Python API routes to the kernels (complex points)
+ODD_FORWARD = False           # odd-factor rfft on the kernels (measured slower than cuFFT)
+RESAMPLE_MIN_LOG2 = 20        # fused resample from max(n, num)/2 = 2^20 (measured faster)
 
 
 MAX_ODD = 15                  # largest odd factor C of a real length n = 2 C 2^e
@@ -52,15 +60,24 @@ def _real_split(n: int) -> tuple[int, int] | None:
     return c, e
 
 
-def _real_in_range(n: int) -> bool:
+def _real_in_range(n: int, inverse: bool = False) -> bool:
     """True when a real transform of length n runs on the kernels: n/2 a power of two in the
-    three-pass range, or C 2^e (C odd <= 15; the C branches run as one batch of packed 2^e-point
-    transforms) with n/2 >= 2^KERNEL_MIN_LOG2."""
+    routed range, or C 2^e (C odd <= 15; the C branches run as one batch of packed 2^e-point
+    transforms) with n/2 >= 2^KERNEL_MIN_LOG2 for the inverse (the forward only with
+    ODD_FORWARD)."""
     sp = _real_split(n)
     if sp is None:
         return False
     c, _ = sp
-    return _pow2_in_range(n // 2) if c == 1 else n // 2 >= (1 << KERNEL_MIN_LOG2)
+    if c == 1:
+        return _pow2_in_range(n // 2)
+    return (inverse or ODD_FORWARD) and n // 2 >= (1 << KERNEL_MIN_LOG2)
+
+
+def _resample_in_range(n: int, num: int) -> bool:
+    """True when a real, unwindowed resample n -> num runs as one fused C-ABI call."""
+    return (_real_split(n) is not None and _real_split(num) is not None
+            and max(n, num) // 2 >= (1 << RESAMPLE_MIN_LOG2))
 
 
 def _notice_long(func_name: str, m: int) -> None:
@@ -162,7 +179,8 @@ def rfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
                    "sp_rfft_c64")
         _watch.record(ws, n // 2, rows, "rfft")
         return _back(out.reshape(batch + (n // 2 + 1,)), axis)
-    _notice_long("rfft", n // 2)
+    if _real_split(n) is None:  # an odd-factor length here is cuFFT by measurement, not a fallback
+        _notice_long("rfft", n // 2)
     return _back(torch.fft.rfft(x, n=n, dim=-1), axis)
 
 
@@ -174,7 +192,7 @@ def irfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
         X = X.to(torch.complex64)
     X = _last(X, axis)
     n = 2 * (X.shape[-1] - 1) if n is None else int(n)
-    if _real_in_range(n):
+    if _real_in_range(n, inverse=True):
         batch = tuple(X.shape[:-1])
         rows = math.prod(batch)
         nb = min(X.shape[-1], n // 2 + 1)
@@ -186,7 +204,8 @@ def irfft(a, n: int | None = None, axis: int = -1) -> torch.Tensor:
                    "sp_irfft_f32")
         _watch.record(ws, n // 2, rows, "irfft")
         return _back(out.reshape(batch + (n,)), axis)
-    _notice_long("irfft", n // 2)
+    if _real_split(n) is None:
+        _notice_long("irfft", n // 2)
     return _back(torch.fft.irfft(X, n=n, dim=-1), axis)
 
 

@@ -6,9 +6,11 @@ fftshift order; a real input's one-sided spectrum takes the window folded onto i
 m = min(num, n) lowest-frequency bins, split (upsampling) or join (downsampling) the unpaired
 bin at m/2 when m is even, scale by num / n and inverse-transform to num samples. Transforms run
 on the three-pass kernels where `mlx_signal_b200.fft` covers their length, cuFFT otherwise.
-A real time-domain input without a window, whose lengths n and num both run on the kernels, takes
-one C-ABI call (`sp_resample_f32`): the forward transform writes only the kept bins, and the bin
-fix-up and the num/n scale are folded into the inverse transform's pretwist.
+A real time-domain input without a window, whose lengths n and num are both 2 C 2^e (C odd <= 15)
+with max(n, num)/2 >= 2^20, takes one C-ABI call (`sp_resample_f32`): the forward transform writes
+only the kept bins, and the bin fix-up and the num/n scale are folded into the inverse transform's
+pretwist (measured by CUDA-graph replay against the same steps on cuFFT: 2^22 -> 3 2^20 71.6 vs
+82.3 us, 3 2^20 -> 2^22 75.2 vs 96.4 us, 2^23 -> 2^22 90.5 vs 117 us).
 """
 
 from __future__ import annotations
@@ -88,8 +90,8 @@ def resample(x, num, t=None, axis=0, window=None, domain="time"):
     m = min(num, n)
     m2 = m // 2 + 1
     W = None if window is None else _freq_window(window, n)
-    if (domain == "time" and not xa.is_complex() and W is None and n > 0
-            and _fft._real_in_range(n) and _fft._real_in_range(num)):
+    if (domain == "time" and not xa.is_complex() and W is None
+            and _fft._resample_in_range(n, num)):
         _fft._watch.poll()
         y = _resample_fused(xa, num)
     elif domain == "time" and not xa.is_complex():

@@ -191,8 +191,8 @@ def test_resample_fused_matches_scipy(rng, monkeypatch, n, num):
     odd-factor lengths, against float64 scipy."""
     from mlx_signal_b200 import fft as bfft
 
-    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
-    assert bfft._real_in_range(n) and bfft._real_in_range(num)
+    monkeypatch.setattr(bfft, "RESAMPLE_MIN_LOG2", 12)
+    assert bfft._resample_in_range(n, num)
     x = rng.standard_normal((2, n)).astype(np.float32)
     ref = sps.resample(x.astype(np.float64), num, axis=-1)
     got = msig.resample(x, num, axis=-1)

@@ -15,9 +15,10 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(autouse=True)
 def kernels_from_2p12(monkeypatch):
-    """These tests exercise the three-pass kernels at every length the C-ABI takes (the public
-    routing sends complex lengths below 2^20 to cuFFT)."""
+    """These tests exercise the kernels at every length the C-ABI takes (the public routing
+    sends complex lengths below 2^22, and odd-factor forward transforms, to cuFFT)."""
     monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
+    monkeypatch.setattr(bfft, "ODD_FORWARD", True)
 
 
 def _rel(got, ref):
@@ -161,7 +162,7 @@ def test_bounded_wait_runs_out_and_reports_timeout(rng, monkeypatch):
     assert _rel(got, np.fft.rfft(xr.cpu().numpy().astype(np.float64))) < 5e-6
 
 
-def test_default_routing_uses_cufft_below_2p20(rng, monkeypatch):
+def test_routing_below_the_threshold_uses_cufft(rng, monkeypatch):
     monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 20)
     assert not bfft._pow2_in_range(1 << 19) and bfft._pow2_in_range(1 << 20)
     x = rng.standard_normal(1 << 14).astype(np.float32)
@@ -215,11 +216,17 @@ def test_odd_factor_structured_and_roundtrip(rng):
 
 
 def test_odd_factor_default_routing(monkeypatch):
-    """With the public threshold (2^20 complex points) a composite real length runs the kernels
-    once n/2 reaches 2^20; odd factors above 15 or packed lengths outside [2^12, 2^26] do not."""
-    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 20)
-    assert bfft._real_in_range(3 << 20) and not bfft._real_in_range(3 << 19)
+    """With the public threshold (2^22 complex points) an odd-factor irfft runs the kernels once
+    n/2 reaches 2^22, the forward stays on cuFFT; odd factors above 15 or packed lengths outside
+    [2^12, 2^26] never run them."""
+    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 22)
+    monkeypatch.setattr(bfft, "ODD_FORWARD", False)
+    assert bfft._real_in_range(3 << 22, inverse=True) and not bfft._real_in_range(3 << 22)
+    assert not bfft._real_in_range(3 << 20, inverse=True)
     assert bfft._real_split(17 << 14) is None and bfft._real_split(3 << 12) is None
+    x = np.random.default_rng(3).standard_normal(3 << 22).astype(np.float32)
+    X = bfft.rfft(x)  # cuFFT
+    assert _rel(bfft.irfft(X, n=3 << 22), x) < 5e-6  # kernels
 
 
 def test_long_transforms_capture_in_a_cuda_graph(rng):

@@ -156,8 +156,13 @@ def test_real_length_split_and_routing(monkeypatch):
     assert bfft._real_split(15 << 13) == (15, 12)
     for n in (0, 1, 3 << 11, 17 << 14, 600_000, (1 << 27) + 2, 1 << 28, 9999):
         assert bfft._real_split(n) is None
-    monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 20)
-    assert bfft._real_in_range(1 << 21) and not bfft._real_in_range(1 << 20)
-    assert bfft._real_in_range(3 << 20) and not bfft._real_in_range(3 << 19)
+    assert bfft.KERNEL_MIN_LOG2 == 22 and not bfft.ODD_FORWARD
+    assert bfft._real_in_range(1 << 23) and not bfft._real_in_range(1 << 22)
+    assert bfft._real_in_range(3 << 22, inverse=True) and not bfft._real_in_range(3 << 22)
+    assert not bfft._real_in_range(3 << 21, inverse=True)
+    assert bfft._resample_in_range(1 << 22, 3 << 20) and bfft._resample_in_range(1 << 21, 3 << 19)
+    assert not bfft._resample_in_range(1 << 20, 3 << 18)
+    assert not bfft._resample_in_range(1 << 22, 1001)
     monkeypatch.setattr(bfft, "KERNEL_MIN_LOG2", 12)
+    monkeypatch.setattr(bfft, "ODD_FORWARD", True)
     assert bfft._real_in_range(3 << 13) and bfft._real_in_range(1 << 13)

@@ -102,6 +102,9 @@ def _blue_stft(msig, k):
 
 
 def _rfft_odd(msig, k):
+    # both directions on the kernels (the public routing sends this forward length to cuFFT)
+    msig.fft.ODD_FORWARD = True
+    msig.fft.KERNEL_MIN_LOG2 = 12
     x = _randn(3 << 20, 12)
     X = msig.fft.rfft(x)
     return [lambda: msig.fft.rfft(x), lambda: msig.fft.irfft(X, n=3 << 20)] * k
