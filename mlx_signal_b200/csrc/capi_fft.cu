@@ -51,12 +51,15 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// digits (R3, R2, R1) of N = 2^e, as balanced as possible (each in [16, 512] for e in [12, 26])
+// digits (R3, R2, R1) of N = 2^e, as balanced as possible (each in [16, 512] for e in [12, 26]);
+// a larger digit goes to pass 1 (R3) first, then pass 2: pass 1 writes its output with direct
+// stores, so its longer columns cost no staging (measured 2^23 rfft 55.8 -> 54.1 us against
+// the longer column in pass 3)
 void digits(int e, int* R3, int* R2, int* R1) {
   const int a = e / 3, rem = e % 3;
-  *R1 = 1 << (a + (rem > 0 ? 1 : 0));
+  *R3 = 1 << (a + (rem > 0 ? 1 : 0));
   *R2 = 1 << (a + (rem > 1 ? 1 : 0));
-  *R3 = 1 << a;
+  *R1 = 1 << a;
 }
 
 // 3-D float32 tensor map over rows of 2*d0 floats: dims {2 d0, d1, d2}, box {32, b1, b2},

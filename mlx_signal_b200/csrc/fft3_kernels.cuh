@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
 // kUntT indices k = k0 + j * kUntB (j < kUntT): one FP64 sincospi anchor at k0, then an FP64
 // rotation by the launch's step d = exp(-i pi kUntB / m) per index, each rounded to FP32 once.
 constexpr int kUntB = 256;  // threads per block
-constexpr int kUntT = 8;    // indices per thread
+constexpr int kUntT = 4;    // indices per thread (8 and 16 measured slower at 2^22)
 
 // Packed real FFT untangle (n = 2m real samples viewed as m complex z, Z = FFT_m(z)):
 //   X_k = (Z_k + conj Z_{m-k})/2 - i w_k (Z_k - conj Z_{m-k})/2, w_k = exp(-i pi k/m), k < m;
