@@ -59,6 +59,18 @@ __global__ void __launch_bounds__(32 * kRedGroups) k_reduce_mean(ReduceParams p)
       const float* q = p.partial + r * p.cmax * int64_t(stride) + kc;
 #pragma unroll 4
       for (int c = grp; c < nsl; c += kRedGroups) a0 += double(q[int64_t(c) * stride]);
+    } else if (p.f64) {
+      const int stride = cross_slot_floats(L);
+      const int cq = cross_q_floats(L);
+      const double* base = reinterpret_cast<const double*>(p.partial) + r * p.cmax * int64_t(stride);
+#pragma unroll 2
+      for (int c = grp; c < nsl; c += kRedGroups) {
+        const double* q = base + int64_t(c) * stride;
+        a0 += q[k];
+        a1 += q[kk];
+        a2 += q[cq + 2 * kc];
+        a3 += q[cq + 2 * kc + 1];
+      }
     } else {
       const int stride = cross_slot_floats(L);
       const int cq = cross_q_floats(L);
@@ -127,6 +139,7 @@ struct MeanPlanInfo {
   int nseg = 0;
   int64_t total = 0, G = 0, nteams = 0, blocks = 0;
   int cmax = 0;
+  bool f64 = false;  // FP64 partial slots (k_cross_mean / k_cross_half)
   int64_t slot_floats = 0;
   int64_t ws_bytes = 0;
 };
@@ -202,7 +215,8 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   int64_t cm = cdiv(pl->nseg, pl->G) + 1;
   if (cm > pl->nteams) cm = pl->nteams;
   pl->cmax = int(cm);
-  pl->slot_floats = cross ? cross_slot_floats(nfft)
+  pl->f64 = cross && !blue;
+  pl->slot_floats = cross ? (pl->f64 ? 2 : 1) * int64_t(cross_slot_floats(nfft))
                           : (mode == 4 ? 2 * int64_t(nfft)
                                        : (cplx ? cross_q_floats(nfft) : welch_slot_floats(nfft)));
   pl->ws_bytes = rows * pl->cmax * pl->slot_floats * int64_t(sizeof(float));
@@ -262,6 +276,7 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   rp.cmax = pl.cmax;
   rp.nteams = pl.nteams;
   rp.mode = mode;
+  rp.f64 = pl.f64 ? 1 : 0;
   rp.out = out;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(rows * cdiv(rp.nout, 32)));

@@ -476,8 +476,77 @@ __host__ __device__ constexpr int cross_slot_floats(int L) {
   return cross_q_floats(L) + 2 * (L / 2 + 1);
 }
 
+// Blocked summation of the cross kernels: each thread sums kFoldSegs segments' terms in FP32
+// registers, then the team adds that block into its FP64 partial slot (a plain store for the
+// first block of a row range, fire-and-forget FP64 reductions after it; only the owning team
+// writes a slot). A team's sum then rounds in FP32 over at most kFoldSegs terms
+// and in FP64 across blocks, whatever the number of segments; k_reduce_mean sums the FP64 slots.
+// (The welch kernels keep their block totals in shared memory; the cross kernels' Q and C
+// accumulators would need about 2 L floats per team there, which would cost a CTA per SM.)
+constexpr int kFoldSegs = 32;
+
+// The block is staged in the team's exchange buffer (free between segments; it holds the
+// slot's 2 L + 2 floats) and added from there by a strided loop, which keeps the FP64 work off
+// the registers of the segment loop.
+template <class PL, int EH1>
+__device__ __forceinline__ void flush_cross_f64(float (&q)[PL::E], float (&cr)[EH1],
+                                                float (&ci)[EH1], double* slot, float2* buf, int t,
+                                                unsigned mask, bool first) {
+  constexpr int L = PL::L, E = PL::E, P = PL::P, CQ = cross_q_floats(L);
+  if constexpr (PL::BUF * 2 < cross_slot_floats(L)) {
+    // short transforms (L < 16: no padding in the exchange buffer): each thread adds its own
+    // elements directly
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      double* d = slot + t + e * P;
+      if (first) *d = double(q[e]);
+      else atomicAdd(d, double(q[e]));
+      q[e] = 0.f;
+    }
+#pragma unroll
+    for (int e = 0; e < EH1; ++e) {
+      if (e < E / 2 || t == 0) {
+        double* d = slot + CQ + 2 * (t + e * P);
+        if (first) {
+          d[0] = double(cr[e]);
+          d[1] = double(ci[e]);
+        } else {
+          atomicAdd(d, double(cr[e]));
+          atomicAdd(d + 1, double(ci[e]));
+        }
+      }
+      cr[e] = ci[e] = 0.f;
+    }
+    if ((L & 1) && t == 0 && first) slot[L] = 0.0;
+    return;
+  }
+  float* sq = reinterpret_cast<float*>(buf);
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    sq[t + e * P] = q[e];
+    q[e] = 0.f;
+  }
+#pragma unroll
+  for (int e = 0; e < EH1; ++e) {
+    if (e < E / 2 || t == 0) {
+      sq[CQ + 2 * (t + e * P)] = cr[e];
+      sq[CQ + 2 * (t + e * P) + 1] = ci[e];
+    }
+    cr[e] = ci[e] = 0.f;
+  }
+  if (L & 1) sq[L] = 0.f;  // the padding float of Q
+  team_sync<P>(mask);
+  if (first) {
+    for (int i = t; i < cross_slot_floats(L); i += P) slot[i] = double(sq[i]);
+  } else {
+    for (int i = t; i < cross_slot_floats(L); i += P) atomicAdd(slot + i, double(sq[i]));
+  }
+  team_sync<P>(mask);
+}
+
 // csd / coherence: z = x_s + i y_s. Accumulates Q_k = sum |Z_k|^2 (all k) and
-// C_k = sum Z_k Z_{L-k} for k in [0, L/2] (C is symmetric in k <-> L-k).
+// C_k = sum Z_k Z_{L-k} for k in [0, L/2] (C is symmetric in k <-> L-k), blocked into FP64
+// partial slots (flush_cross_f64).
 template <int LOG_L, int LOG_E, int DET>
 __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
     k_cross_mean(MeanParams pr) {
@@ -493,11 +562,11 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
   float q[E];
-  float2 c[EH];
+  float cr[EH], ci[EH];
 #pragma unroll
   for (int e = 0; e < E; ++e) q[e] = 0.f;
 #pragma unroll
-  for (int e = 0; e < EH; ++e) c[e] = make_float2(0.f, 0.f);
+  for (int e = 0; e < EH; ++e) cr[e] = ci[e] = 0.f;
   while (g < gend) {
     const int64_t r = g / pr.nseg;
     const int s0 = int(g - r * pr.nseg);
@@ -505,6 +574,11 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
     const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
     const float* xr = pr.x + r * pr.ld_x;
     const float* yr = pr.y + r * pr.ld_y;
+    const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
+    double* dslot = reinterpret_cast<double*>(pr.partial) +
+                    (r * pr.cmax + slot) * int64_t(cross_slot_floats(L));
+    bool first = true;
+    int nblk = 0;
     for (int s = s0; s < s1; ++s) {
       float2 v[E];
       load_pair<PL>(v, xr + int64_t(s) * pr.hop, yr + int64_t(s) * pr.hop, true, t, pr.nperseg);
@@ -527,25 +601,18 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
         if (e < E / 2 || t == 0) {
           const int k = t + e * P;
           const float2 m = buf[PL::pad((L - k) & (L - 1))];
-          c[e].x = fmaf(v[e].x, m.x, fmaf(-v[e].y, m.y, c[e].x));
-          c[e].y = fmaf(v[e].x, m.y, fmaf(v[e].y, m.x, c[e].y));
+          cr[e] = fmaf(v[e].x, m.x, fmaf(-v[e].y, m.y, cr[e]));
+          ci[e] = fmaf(v[e].x, m.y, fmaf(v[e].y, m.x, ci[e]));
         }
       }
       team_sync<P>(mask);
+      if (++nblk == kFoldSegs) {
+        flush_cross_f64<PL, EH>(q, cr, ci, dslot, buf, t, mask, first);
+        first = false;
+        nblk = 0;
+      }
     }
-    const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
-    float* dst = pr.partial + (r * pr.cmax + slot) * int64_t(cross_slot_floats(L));
-    float2* dstc = reinterpret_cast<float2*>(dst + cross_q_floats(L));
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      dst[t + e * P] = q[e];
-      q[e] = 0.f;
-    }
-#pragma unroll
-    for (int e = 0; e < EH; ++e) {
-      if (e < E / 2 || t == 0) dstc[t + e * P] = c[e];
-      c[e] = make_float2(0.f, 0.f);
-    }
+    if (first || nblk) flush_cross_f64<PL, EH>(q, cr, ci, dslot, buf, t, mask, first);
     g += s1 - s0;
   }
 }
@@ -556,9 +623,9 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS)
 // table; the segment means come from the carried half-block sum plus the new one; the constant
 // detrend runs inside the fused stage (DET == kDetrendConstant) or as the low-bin spectral
 // correction Z_k -= (m_x + i m_y) DFT(win)_k (DET == kDetrendConstantSpectral); the next
-// half-block is prefetched into L2. Partial slots are those of k_cross_mean (Q_k for all k,
-// C_k = Z_k Z_{L-k} for k <= L/2); CSD accumulates only Im C (its real part is stored as zero:
-// csd does not read it).
+// half-block is prefetched into L2. Partial slots are those of k_cross_mean (FP64 Q_k for all k,
+// C_k = Z_k Z_{L-k} for k <= L/2, blocked every kFoldSegs segments); CSD accumulates only Im C
+// (its real part stays zero: csd does not read it).
 template <int LOG_L, int LOG_E, int DET, bool CSD>
 __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L, LOG_E>::MIN_CTAS)
     k_cross_half(MeanParams pr) {
@@ -609,6 +676,11 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
     const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
     const float* xr = pr.x + r * pr.ld_x;
     const float* yr = pr.y + r * pr.ld_y;
+    const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
+    double* dslot = reinterpret_cast<double*>(pr.partial) +
+                    (r * pr.cmax + slot) * int64_t(cross_slot_floats(L));
+    bool first = true;
+    int nblk = 0;
     float sax = 0.f, say = 0.f;  // sums of this segment's A half (the previous B)
     bool have_a = false;
     for (int s = s0; s < s1; ++s) {
@@ -709,20 +781,13 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
         }
       }
       team_sync<P>(mask);
+      if (++nblk == kFoldSegs) {
+        flush_cross_f64<PL, EH1>(q, cr, ci, dslot, buf, t, mask, first);
+        first = false;
+        nblk = 0;
+      }
     }
-    const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
-    float* dst = pr.partial + (r * pr.cmax + slot) * int64_t(cross_slot_floats(L));
-    float2* dstc = reinterpret_cast<float2*>(dst + cross_q_floats(L));
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      dst[t + e * P] = q[e];
-      q[e] = 0.f;
-    }
-#pragma unroll
-    for (int e = 0; e < EH1; ++e) {
-      if (e < E / 2 || t == 0) dstc[t + e * P] = make_float2(CSD ? 0.f : cr[e], ci[e]);
-      cr[e] = ci[e] = 0.f;
-    }
+    if (first || nblk) flush_cross_f64<PL, EH1>(q, cr, ci, dslot, buf, t, mask, first);
     g += s1 - s0;
   }
 }
@@ -740,6 +805,7 @@ struct ReduceParams {
   int cmax;
   int64_t nteams;
   int mode;
+  int f64;           // modes 1/2: FP64 partial slots (k_cross_mean / k_cross_half)
   float* out;
 };
 

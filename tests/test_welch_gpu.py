@@ -502,6 +502,42 @@ def test_welch_long_channel_segment_sums():
     assert rel_err_bins(p.cpu().numpy(), pref) <= 1e-5
 
 
+def _csd_f64_chunked(x, y, nperseg, chunk_segments=1 << 15):
+    """float64 scipy csd of two long 1-D signals over blocks of whole segments (as above)."""
+    hop = nperseg // 2
+    nseg = (x.shape[0] - nperseg) // hop + 1
+    total = None
+    for s0 in range(0, nseg, chunk_segments):
+        s1 = min(nseg, s0 + chunk_segments)
+        sl = slice(s0 * hop, (s1 - 1) * hop + nperseg)
+        f, p = sps.csd(x[sl].astype(np.float64), y[sl].astype(np.float64), nperseg=nperseg)
+        total = p * (s1 - s0) if total is None else total + p * (s1 - s0)
+    return f, total / nseg
+
+
+def test_cross_long_channel_segment_sums():
+    """csd and coherence of one 2^26-sample pair at nperseg 256 (524287 segments in one row):
+    each team's FP32 sums are flushed into FP64 partial slots every 32 segments, and both stay
+    within 1e-5 relative of float64 scipy on bins above 1e-6 of the peak (tone plus noise, y a
+    delayed noisy copy of x)."""
+    n = 1 << 26
+    g = torch.Generator(device="cuda")
+    g.manual_seed(27)
+    x = torch.randn(n, generator=g, device="cuda")
+    t = torch.arange(n, device="cuda", dtype=torch.float64)
+    x += (3.0 * torch.sin(2 * np.pi * 0.123 * t)).float()
+    y = 0.7 * torch.roll(x, 17) + 0.3 * torch.randn(n, generator=g, device="cuda")
+    _, pxy = msig.csd(x, y, nperseg=256)
+    _, coh = msig.coherence(x, y, nperseg=256)
+    xh, yh = x.cpu().numpy(), y.cpu().numpy()
+    _, ref_xy = _csd_f64_chunked(xh, yh, 256)
+    assert rel_err_bins(pxy.cpu().numpy(), ref_xy) <= 1e-5
+    _, ref_xx = _welch_f64_chunked(xh, 256)
+    _, ref_yy = _welch_f64_chunked(yh, 256)
+    ref_coh = np.abs(ref_xy) ** 2 / (ref_xx * ref_yy)
+    assert rel_err_bins(coh.cpu().numpy(), ref_coh) <= 1e-5
+
+
 @pytest.mark.parametrize("kw", [
     {"nperseg": 8192},
     {"nperseg": 8192, "detrend": "linear"},
