@@ -148,12 +148,24 @@ struct MeanPlanInfo {
 // bins k < P and k > L - P are the first and last register of every team thread.
 int spectral_bins(int log_l) { return (1 << log_l) >> team_log_e_rt(log_l); }
 
+// CTA waves of the 50%-overlap welch and csd / coherence grids at short segments. With one team
+// range per resident team, the SMs of the 64 x 2^20 welch at nperseg 256 finished between 57 %
+// and 100 % of the kernel's time (identical team ranges; ncu sm__cycles_active min/max); shorter
+// ranges over several waves let the block scheduler even that out. Measured on 64 x 2^20 (welch,
+// 1 / 2 / 4 / 8 waves, us): nperseg 32 315 / 330 / 369 / 423, 64 182 / 164 / 161 / 175,
+// 128 186 / 162 / 164 / 173, 256 151 / 133 / 127 / 137, 512 144 / 144 / 147 / 155 (1024 and up
+// lose to the extra per-CTA setup); csd pairs with this rule at nperseg 64 / 128 / 256:
+// 498 / 452 / 381 -> 463 / 408 / 317 us.
+int half_waves(int log_l) { return log_l == 8 ? 4 : (log_l == 6 || log_l == 7) ? 2 : 1; }
+
 // mode: 0 welch, 1 csd, 2 coherence. The segments-per-team split (and so the workspace size)
 // comes from one canonical kernel per family (the time-domain-detrend variant, coherence for the
 // cross family), so sp_mean_workspace_size, which knows neither the detrend form nor csd vs
 // coherence, sizes every variant's launch.
+// fine = false keeps one wave (the smallest workspace; the no-allocation entry point falls back
+// to it when the finer split's partial slots would not fit its fixed scratch).
 int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop, int detrend,
-              MeanPlanInfo* pl, bool spectral = false) {
+              MeanPlanInfo* pl, bool spectral = false, bool fine = true) {
   // mode 3: welch of complex rows (one segment per transform, two-sided); mode 4: csd of two
   // complex signals (two transforms per segment, two-sided)
   const bool cplx = mode == 3 || mode == 4;
@@ -208,7 +220,10 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   }
   const int64_t cap = int64_t(nb) * sms * canon.teams;
   const int64_t total = pl->total > 0 ? pl->total : 1;
-  pl->G = (cross || cplx) ? cdiv(total, cap) : 2 * cdiv(total, 2 * cap);
+  const int waves = (fine && half) ? half_waves(log_l) : 1;
+  pl->G = cplx    ? cdiv(total, cap)
+          : cross ? cdiv(total, int64_t(waves) * cap)
+                  : 2 * cdiv(total, 2 * int64_t(waves) * cap);
   if (pl->G < 1) pl->G = 1;
   pl->nteams = cdiv(total, pl->G);
   pl->blocks = cdiv(pl->nteams, pl->k.teams);
@@ -226,7 +241,7 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
 int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, int64_t ldx,
              int64_t ldy, const float* win, int nperseg, int nfft, int hop, int detrend,
              int onesided, float* out, void* ws, size_t ws_bytes, void* stream,
-             const float* wdft = nullptr, int n_low = 0) {
+             const float* wdft = nullptr, int n_low = 0, bool fine = true) {
   const bool cross = mode == 1 || mode == 2 || mode == 4;  // two input signals
   if (!x || !win || !out || (cross && !y) || ldx < n || (cross && ldy < n)) {
     set_error("null pointer or row stride smaller than n");
@@ -236,7 +251,7 @@ int run_mean(int mode, const float* x, const float* y, int64_t rows, int64_t n, 
   const bool spectral = wdft != nullptr && n_low >= 1 && log_l_in >= 1 &&
                         n_low <= spectral_bins(log_l_in);
   MeanPlanInfo pl;
-  int st = make_plan(mode, rows, n, nperseg, nfft, hop, detrend, &pl, spectral);
+  int st = make_plan(mode, rows, n, nperseg, nfft, hop, detrend, &pl, spectral, fine);
   if (st != SP_OK) return st;
   if (rows == 0) return SP_OK;
   if (ws_bytes < size_t(pl.ws_bytes) || (pl.ws_bytes > 0 && !ws)) {
@@ -365,8 +380,14 @@ int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld, co
                          int nperseg, int nfft, int hop, int detrend, int onesided, float* out,
                          void* stream) {
   b2s::MeanPlanInfo pl;
-  const int st = b2s::make_plan(0, rows, n, nperseg, nfft, hop, detrend, &pl);
+  int st = b2s::make_plan(0, rows, n, nperseg, nfft, hop, detrend, &pl);
   if (st != SP_OK) return st;
+  bool fine = true;
+  if (size_t(pl.ws_bytes) > b2s::kNoAllocScratchBytes) {  // one wave needs the least scratch
+    fine = false;
+    st = b2s::make_plan(0, rows, n, nperseg, nfft, hop, detrend, &pl, false, false);
+    if (st != SP_OK) return st;
+  }
   if (size_t(pl.ws_bytes) > b2s::kNoAllocScratchBytes) {
     b2s::set_error(
         "sp_welch_f32_noalloc: this shape needs %lld bytes of scratch but the built-in scratch "
@@ -378,7 +399,7 @@ int sp_welch_f32_noalloc(const float* x, int64_t rows, int64_t n, int64_t ld, co
   const int sst = b2s::noalloc_scratch(&ws);
   if (sst != SP_OK) return sst;
   return b2s::run_mean(0, x, nullptr, rows, n, ld, 0, win, nperseg, nfft, hop, detrend, onesided,
-                       out, ws, b2s::kNoAllocScratchBytes, stream);
+                       out, ws, b2s::kNoAllocScratchBytes, stream, nullptr, 0, fine);
 }
 
 int64_t sp_mean_workspace_size(int kind, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
