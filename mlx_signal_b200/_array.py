@@ -16,10 +16,24 @@ import torch
 from ._config import DowncastWarning, get_config
 
 
+_cuda_ready = False
+
+
+def current_index() -> int:
+    """Index of torch's current CUDA device. After the first successful check this is one call
+    into torch's C extension: the public torch.cuda helpers re-validate availability (environment
+    and driver queries) on every call, which cost ~15 us of host time per spectral call."""
+    global _cuda_ready
+    if not _cuda_ready:
+        if not torch.cuda.is_available():
+            raise RuntimeError("mlx_signal_b200 needs a CUDA device (there is no CPU path)")
+        torch.cuda.init()
+        _cuda_ready = True
+    return torch._C._cuda_getDevice()
+
+
 def device() -> torch.device:
-    if not torch.cuda.is_available():
-        raise RuntimeError("mlx_signal_b200 needs a CUDA device (there is no CPU path)")
-    return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cuda", current_index())
 
 
 def _downcast_notice(src: str) -> None:
@@ -124,5 +138,7 @@ def input_shape(x) -> tuple[int, ...]:
 
 
 def stream_handle() -> int:
-    """Raw cudaStream_t of torch's current stream on the current device."""
-    return torch.cuda.current_stream().cuda_stream
+    """Raw cudaStream_t of torch's current stream on the current device (read through torch's C
+    extension: the same value as torch.cuda.current_stream().cuda_stream without its per-call
+    availability checks)."""
+    return torch._C._cuda_getCurrentRawStream(current_index())

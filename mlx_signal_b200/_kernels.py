@@ -62,21 +62,25 @@ def _workspace(nbytes: int, dev: torch.device) -> torch.Tensor:
 
 
 def welch_mean(x: torch.Tensor, win: torch.Tensor, nperseg: int, nfft: int, hop: int,
-               detrend: int, onesided: bool, wdft: torch.Tensor | None = None) -> torch.Tensor:
+               detrend: int, onesided: bool, wdft: torch.Tensor | None = None,
+               ws: torch.Tensor | None = None) -> torch.Tensor:
     """Mean |FFT(win * detrend(segment))|^2 over segments of each row of x -> (rows, nout).
 
     `wdft` (optional, complex64 CUDA): the non-zero low bins DFT_nfft(win)[0..n_low) of a window
     whose spectrum vanishes elsewhere; lets the constant detrend run as a spectral correction.
+    `ws` (optional): a workspace of at least sp_mean_workspace_size bytes that no other stream
+    uses meanwhile (the caller's plan keeps one per stream); allocated here when absent.
     """
     x, ld = _rows(x)
     rows, n = x.shape
     lib = _lib.load()
-    ws_bytes = lib.sp_mean_workspace_size(0, rows, n, nperseg, nfft, hop, detrend)
-    if ws_bytes < 0:
-        _lib.check(int(ws_bytes), "sp_mean_workspace_size")
+    if ws is None:
+        ws_bytes = lib.sp_mean_workspace_size(0, rows, n, nperseg, nfft, hop, detrend)
+        if ws_bytes < 0:
+            _lib.check(int(ws_bytes), "sp_mean_workspace_size")
+        ws = _workspace(ws_bytes, x.device)
     nout = nfft // 2 + 1 if onesided else nfft
     out = torch.empty((rows, nout), dtype=torch.float32, device=x.device)
-    ws = _workspace(ws_bytes, x.device)
     if wdft is not None:
         _lib.check(
             lib.sp_welch_f32_ex(x.data_ptr(), rows, n, ld, win.data_ptr(), wdft.data_ptr(),

@@ -28,8 +28,9 @@ import warnings
 import numpy as np
 import torch
 
-from . import _kernels
-from ._array import device, input_shape, input_size, to_device, to_numpy
+from . import _kernels, _lib
+from ._array import (current_index, device, input_shape, input_size, stream_handle, to_device,
+                     to_numpy)
 from ._config import composed_path_notice
 from .windows import DEVICE_CONSTANTS, _window_np, device_vector
 
@@ -444,11 +445,26 @@ class _WelchPlan:
         self.geom = (s.nperseg, s.nfft, s.nstep, s.code, s.onesided)
         self.rows, self.n, self.outer, self.axis = rows, n, outer, s.axis
         self.freqs = s.freqs.clone()
+        nb = _lib.load().sp_mean_workspace_size(0, rows, n, s.nperseg, s.nfft, s.nstep, s.code)
+        if nb < 0:
+            _lib.check(int(nb), "sp_mean_workspace_size")
+        self.ws_bytes = max(int(nb), 1)
+        self.ws: dict = {}  # stream handle -> workspace: calls on one stream are ordered
 
     def run(self, x: torch.Tensor):
         X = x.movedim(self.axis, -1) if x.dim() > 1 and self.axis != -1 else x
+        if torch._C._cuda_isCurrentStreamCapturing():  # a captured graph keeps its own
+            ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=x.device)
+        else:
+            st = stream_handle()
+            ws = self.ws.get(st)
+            if ws is None:
+                if len(self.ws) >= 8:
+                    self.ws.clear()
+                ws = self.ws[st] = torch.empty(self.ws_bytes, dtype=torch.uint8,
+                                               device=x.device)
         res = _kernels.welch_mean(X.reshape(self.rows, self.n), self.win, *self.geom,
-                                  wdft=self.wdft)
+                                  wdft=self.wdft, ws=ws)
         pxy = res.reshape(self.outer + (res.shape[-1],))
         if pxy.dim() > 1 and self.axis != -1:
             pxy = pxy.movedim(-1, self.axis if self.axis >= 0 else pxy.dim() + self.axis)
@@ -465,7 +481,7 @@ def _plan_key(x, same, fs, window, nperseg, noverlap, nfft, detrend, return_ones
     if not (same and average == "mean" and isinstance(x, torch.Tensor) and x.is_cuda
             and x.dtype == torch.float32 and isinstance(window, str | tuple)):
         return None
-    if x.device != device():
+    if x.get_device() != current_index():
         return None
     key = (tuple(x.shape), x.device.index, fs, window, nperseg, noverlap, nfft,
            type(detrend).__name__, detrend, return_onesided, scaling, axis)
