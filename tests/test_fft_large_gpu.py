@@ -244,3 +244,17 @@ def test_long_transforms_capture_in_a_cuda_graph(rng):
             assert _rel(got, 2.0 * x.astype(np.float64)) < 5e-6
         del call
     assert bfft.device_status() == 0
+
+
+@pytest.mark.parametrize("e", [22, 23])
+def test_rfft_batched_rows(rng, e):
+    """A batch of 2^22- and 2^23-sample rows through the packed three-pass transform against
+    float64 numpy, and the inverse."""
+    n = 1 << e
+    x = rng.standard_normal((3, n)).astype(np.float32)
+    ref = np.fft.rfft(x.astype(np.float64), axis=-1)
+    got = bfft.rfft(x)
+    for i in range(3):
+        assert _rel(got[i], ref[i]) < 5e-6
+    assert _rel(bfft.irfft(got, n=n), x) < 5e-6
+    assert bfft.device_status() == 0
