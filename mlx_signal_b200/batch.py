@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from . import _kernels, _lib
-from ._array import device, to_device
+from ._array import current_index, device, stream_handle, to_device
 from .autotune import default_cache
 from .windows import _window_np
 
@@ -120,7 +120,7 @@ def _tables(window, nperseg: int) -> _Tables | None:
     key = _window_key(window)
     if key is None:
         return None
-    dev = torch.cuda.current_device()
+    dev = current_index()
     k = (key, int(nperseg), dev)
     hit = _TABLES.get(k)
     if hit is not None:
@@ -423,7 +423,7 @@ class BatchLauncher:
     def _run(self, slot: _Slot) -> None:
         slot.desc_dev.copy_(slot.desc_host, non_blocking=True)
         _lib.check(self.lib.sp_batch_run(slot.desc_dev.data_ptr(), slot.ws.data_ptr(),
-                                         self.grid, torch.cuda.current_stream().cuda_stream),
+                                         self.grid, stream_handle()),
                    "sp_batch_run")
 
     def launch(self, reqs, wait_events=(), keep=None) -> torch.cuda.Event:
@@ -441,7 +441,7 @@ class BatchLauncher:
         _lib.check(self.lib.sp_batch_encode(addr, count, slot.ws.data_ptr(), slot.ws.numel(),
                                             slot.desc_host.data_ptr(), self.desc_bytes),
                    "sp_batch_encode")
-        cur = torch.cuda.current_stream()
+        cur = torch.cuda.current_stream(current_index())
         slot.stream.wait_stream(cur)  # inputs produced on the caller's stream
         for ev in wait_events:
             slot.stream.wait_event(ev)
@@ -511,8 +511,8 @@ def welch_batch(signals, **kwargs):
                                        host.numel()), "sp_batch_encode")
         # torch's pinned-memory allocator holds `host` until the copy has run
         desc = host.to(dev, non_blocking=True)
-        _lib.check(lib.sp_batch_run(desc.data_ptr(), ws.data_ptr(), 0,
-                                    torch.cuda.current_stream().cuda_stream), "sp_batch_run")
+        _lib.check(lib.sp_batch_run(desc.data_ptr(), ws.data_ptr(), 0, stream_handle()),
+                   "sp_batch_run")
     out = []
     for (x, kw), j in zip(items, jobs):
         if j is not None:

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _kernels, _lib, batch
-from ._array import device, to_device
+from ._array import device, stream_handle, to_device
 from .spectral import _detrend_code, _freqs, stft, welch
 from .windows import _window_np, device_vector
 
@@ -78,8 +78,8 @@ class StreamingSTFT:
                                        host.data_ptr(), host.numel()), "sp_batch_encode")
         # torch's pinned-memory allocator holds `host` until the copy has run
         desc = host.to(device(), non_blocking=True)
-        _lib.check(lib.sp_batch_run(desc.data_ptr(), self._ws.data_ptr(), 0,
-                                    torch.cuda.current_stream().cuda_stream), "sp_batch_run")
+        _lib.check(lib.sp_batch_run(desc.data_ptr(), self._ws.data_ptr(), 0, stream_handle()),
+                   "sp_batch_run")
         return job.result()
 
     def _push_frames(self, X: torch.Tensor):
