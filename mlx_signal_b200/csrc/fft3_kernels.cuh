@@ -15,10 +15,11 @@
 //    (cp.async.bulk.tensor, 128B swizzle, mbarrier completion, no multicast), so the strided
 //    column walk of the reference's per-thread gather becomes one coalesced bulk transfer;
 //  * each tile column is an L-point team FFT in registers (the spectral kernels' engine);
-//  * inter-pass twiddles come from per-tile shared-memory tables filled while the tile's copy
-//    is in flight, each entry an FP64 sincospi of the exactly reduced integer phase rounded to
-//    FP32 once (pass 1: one per output row; pass 2: one per row and one per column, multiplied
-//    per element in FP32) -- no twiddle table in global memory;
+//  * inter-pass twiddles are formed in FP64 and rounded to FP32 once: pass 1 from a per-tile
+//    shared-memory table (an FP64 sincospi of the exactly reduced integer phase per output row,
+//    filled while the tile's copy is in flight), pass 2 per thread from an FP64 anchor and step
+//    (sincospi of exact integer phases) and an FP64 recurrence over the thread's rows -- no
+//    twiddle table in global memory;
 //  * the inverse transform is conj(FFT(conj(x))) / N with 1/N folded into pass 1.
 // Every mbarrier wait is bounded; on timeout the CTA records SP_ERR_TIMEOUT in the error word,
 // waits (bounded) for its own copies and returns without touching the data; the code is also
@@ -243,21 +244,13 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
     //   pass 2: W_N^(r km2 R3) per row km2 and W_N^(r km3) per column km3, multiplied per
     //           element in FP32 (about one ulp more than a product rounded once; no FP64 work
     //           per element).
-    if constexpr (PASS != 3) {
+    if constexpr (PASS == 1) {
       int cg_, slab_, b_;
       fft3_tile_coords<PASS>(tl, R1, R2, R3, &cg_, &slab_, &b_);
-      if constexpr (PASS == 1) {
-        const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
-        for (int i = threadIdx.x; i < L; i += blockDim.x) {
-          const double2 w = w_exact(int64_t(R1) * slab_ * i, N);
-          ttw[i] = make_float2(float(w.x * sc), float(w.y * sc));
-        }
-      } else {
-        for (int i = threadIdx.x; i < L + kTileCols; i += blockDim.x) {
-          const double2 w = i < L ? w_exact(int64_t(slab_) * i * R3, N)
-                                  : w_exact(int64_t(slab_) * (cg_ * kTileCols + (i - L)), N);
-          ttw[i] = make_float2(float(w.x), float(w.y));
-        }
+      const double sc = pr.inverse ? 1.0 / double(N) : 1.0;
+      for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        const double2 w = w_exact(int64_t(R1) * slab_ * i, N);
+        ttw[i] = make_float2(float(w.x * sc), float(w.y * sc));
       }
     }
     const bool ok = __syncthreads_and(mbar_wait(bar + j, par, pr.wait_polls) ? 1 : 0) != 0;
@@ -304,10 +297,17 @@ __global__ void __launch_bounds__(Fft3Cfg<LOG_L, LOG_E>::THREADS,
       for (int e = 0; e < E; ++e) dst[t + e * P] = cmul(v[e], ttw[t + e * P]);
     } else {
       if constexpr (PASS == 2) {
-        // twiddle W_N^(r (km2 R3 + km3)) = W_N^(r km2 R3) W_N^(r km3), km2 = t + e P
-        const float2 wc = ttw[L + c];
+        // twiddle W_N^(r (km2 R3 + km3)), km2 = t + e P, km3 = col0 + c: an FP64 anchor
+        // W_N^(r (t R3 + km3)) and step W_N^(r R3 P), an FP64 recurrence over e, each factor
+        // rounded to FP32 once
+        const int64_t r = slab, km3 = col0 + c;
+        double2 w = w_exact(r * (int64_t(t) * R3 + km3), N);
+        const double2 st = w_exact(r * R3 * P, N);
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = cmul(v[e], cmul(ttw[t + e * P], wc));
+        for (int e = 0; e < E; ++e) {
+          v[e] = cmul(v[e], make_float2(float(w.x), float(w.y)));
+          w = zmul(w, st);
+        }
       }
       __syncthreads();  // every team has read its column: the tile can be overwritten
   #pragma unroll
