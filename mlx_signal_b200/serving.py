@@ -112,6 +112,10 @@ class SpectralServer:
         self.frames_emitted = np.zeros(self.max_streams, np.int64)
         self.busy = np.zeros(self.max_streams, bool)
         self.pending: collections.deque[_Pending] = collections.deque()
+        # stream chunks that wait behind an earlier chunk of their stream (in flight, chosen for
+        # the batch being built, or itself waiting), per stream in arrival order; streams in the
+        # order their first waiting chunk arrived
+        self.held: dict[int, collections.deque[_Pending]] = {}
         self.inflight: collections.deque = collections.deque()
         self.used = 0
         self.next_rid = 0
@@ -189,19 +193,43 @@ class SpectralServer:
             self.stats.completed += len(reqs)
             self.stats.last_done = now
 
+    def queued(self) -> bool:
+        """True while some submitted request has not been launched."""
+        return bool(self.pending) or bool(self.held)
+
     def _select(self) -> list[_Pending]:
-        """FIFO admission: requests in arrival order while the batch and the budget have room;
-        a chunk of a stream that has a chunk in flight (or earlier in this batch) waits."""
+        """FIFO admission while the batch and the budget have room. Waiting chunks of streams
+        that are free again go first (they arrived before anything still pending); a chunk of a
+        stream with a chunk in flight, in this batch or already waiting moves once to that
+        stream's held queue, so one selection costs O(streams + batch), not a rescan of the
+        backlog."""
         chosen = []
-        deferred = []
         room = self.budget - self.used
         taken = set()
+        for s in list(self.held):
+            if len(chosen) >= self.max_batch:
+                return chosen
+            if self.busy[s]:
+                continue
+            q = self.held[s]
+            r = q[0]
+            if r.nbytes > room:
+                return chosen
+            q.popleft()
+            if not q:
+                del self.held[s]
+            chosen.append(r)
+            room -= r.nbytes
+            taken.add(s)
         while self.pending and len(chosen) < self.max_batch:
             r = self.pending[0]
-            if r.kind == KIND_STREAM and (self.busy[r.stream] or r.stream in taken):
-                deferred.append(self.pending.popleft())
-                if len(deferred) > 4 * self.max_batch:
-                    break
+            if r.kind == KIND_STREAM and (self.busy[r.stream] or r.stream in taken
+                                          or r.stream in self.held):
+                self.pending.popleft()
+                q = self.held.get(r.stream)
+                if q is None:
+                    q = self.held[r.stream] = collections.deque()
+                q.append(r)
                 continue
             if r.nbytes > room:
                 break
@@ -210,8 +238,6 @@ class SpectralServer:
             room -= r.nbytes
             if r.kind == KIND_STREAM:
                 taken.add(r.stream)
-        for r in reversed(deferred):
-            self.pending.appendleft(r)
         return chosen
 
     def _launch(self, reqs: list[_Pending]) -> None:
@@ -297,7 +323,7 @@ class SpectralServer:
         of requests launched."""
         now = time.perf_counter()
         self._retire(now)
-        if not self.pending or len(self.inflight) >= len(self.launcher.slots):
+        if not self.queued() or len(self.inflight) >= len(self.launcher.slots):
             return 0
         reqs = self._select()
         if not reqs:
@@ -309,7 +335,7 @@ class SpectralServer:
 
     def drain(self) -> None:
         """Run the loop until every submitted request has completed."""
-        while self.pending or self.inflight:
+        while self.queued() or self.inflight:
             if self.step() == 0 and self.inflight:
                 self.inflight[0][0].synchronize()
         self._retire(time.perf_counter())
@@ -386,7 +412,7 @@ def run_schedule(server: SpectralServer, schedule) -> ServerStats:
         t0 = time.perf_counter()
         i = 0
         n = len(schedule)
-        while i < n or server.pending or server.inflight:
+        while i < n or server.queued() or server.inflight:
             now = time.perf_counter()
             while i < n and t0 + schedule[i][0] <= now:
                 arr, kind, x, p = schedule[i]
