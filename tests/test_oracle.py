@@ -117,7 +117,7 @@ def test_pair_trick_identities(rng):
 
 
 def test_group_params_match_reference_rule():
-    # 64 channels x 2047 segments -> groups of 64, 32 per row (the survey's worked example)
+    # 64 channels x 2047 segments (the 64 x 2^20, nperseg 1024 welch) -> groups of 64, 32 per row
     assert restate.group_params(64, 2047) == (64, 32)
     assert restate.group_params(2048, 9) == (9, 1)
     assert restate.group_params(1, 1) == (1, 1)
