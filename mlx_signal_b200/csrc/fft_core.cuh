@@ -290,6 +290,11 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
     constexpr int pn = p + 1;
     constexpr int Rn = PL::radix(pn), Sn = PL::span(pn), Bn = PL::E / Rn;
     const float2* twp = tw + PL::tw_off(pn);
+    // Radix-16 passes of transforms of 2048 points and more (exchange- and twiddle-read-bound
+    // in shared memory) read the twiddle anchors w, w^2, w^4, w^8 of the butterfly and form the
+    // other eleven powers by complex products in registers (each within ~2 ulp), a quarter of
+    // the twiddle reads.
+    constexpr bool kAnchors = L >= 2048 && Rn == 16;
     static_for<0, Bn>([&](auto bc) {
       constexpr int b = decltype(bc)::value;
       const int j = t + P * b;
@@ -298,6 +303,17 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
       // offset from pad(j)
       constexpr int QS = L / Rn;
       const float2* pj = buf + PL::pad(j);
+      float2 w1, w2, w3, w4, w5, w6, w7, w8;
+      if constexpr (kAnchors) {
+        w1 = twp[Sn + jm];
+        w2 = twp[2 * Sn + jm];
+        w4 = twp[4 * Sn + jm];
+        w8 = twp[8 * Sn + jm];
+        w3 = cmul(w1, w2);
+        w5 = cmul(w4, w1);
+        w6 = cmul(w4, w2);
+        w7 = cmul(w4, w3);
+      }
       static_for<0, Rn>([&](auto qc) {
         constexpr int q = decltype(qc)::value;
         float2 val;
@@ -306,7 +322,17 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
         } else {
           val = buf[PL::pad(j + q * QS)];
         }
-        if constexpr (q > 0) val = cmul(val, twp[q * Sn + jm]);
+        if constexpr (q > 0) {
+          if constexpr (kAnchors) {
+            constexpr int lo = q & 7;
+            const float2 wl = lo == 1 ? w1 : lo == 2 ? w2 : lo == 3 ? w3 : lo == 4 ? w4
+                            : lo == 5 ? w5 : lo == 6 ? w6 : w7;
+            const float2 wq = q == 8 ? w8 : (q > 8 ? cmul(w8, wl) : wl);
+            val = cmul(val, wq);
+          } else {
+            val = cmul(val, twp[q * Sn + jm]);
+          }
+        }
         v[b * Rn + bitrev(q, ilog2(Rn))] = val;
       });
     });
