@@ -17,6 +17,10 @@ from ._config import DowncastWarning, get_config
 
 
 _cuda_ready = False
+# torch's C-extension accessors for the current device and raw stream (present in the torch
+# releases this package is built against); the public helpers below are the fallback
+_get_device = getattr(torch._C, "_cuda_getDevice", None)
+_get_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
 
 
 def current_index() -> int:
@@ -29,7 +33,7 @@ def current_index() -> int:
             raise RuntimeError("mlx_signal_b200 needs a CUDA device (there is no CPU path)")
         torch.cuda.init()
         _cuda_ready = True
-    return torch._C._cuda_getDevice()
+    return _get_device() if _get_device is not None else torch.cuda.current_device()
 
 
 def device() -> torch.device:
@@ -141,4 +145,6 @@ def stream_handle() -> int:
     """Raw cudaStream_t of torch's current stream on the current device (read through torch's C
     extension: the same value as torch.cuda.current_stream().cuda_stream without its per-call
     availability checks)."""
-    return torch._C._cuda_getCurrentRawStream(current_index())
+    if _get_raw_stream is not None:
+        return _get_raw_stream(current_index())
+    return torch.cuda.current_stream(current_index()).cuda_stream

@@ -453,7 +453,7 @@ class _WelchPlan:
 
     def run(self, x: torch.Tensor):
         X = x.movedim(self.axis, -1) if x.dim() > 1 and self.axis != -1 else x
-        if torch._C._cuda_isCurrentStreamCapturing():  # a captured graph keeps its own
+        if torch.cuda.is_current_stream_capturing():  # a captured graph keeps its own
             ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=x.device)
         else:
             st = stream_handle()
