@@ -451,11 +451,14 @@ SP_API int sp_batch_plan(const sp_batch_request* reqs, int nreq, int64_t* desc_b
 SP_API int sp_batch_encode(const sp_batch_request* reqs, int nreq, void* ws, size_t ws_bytes,
                            void* desc_host, size_t desc_bytes);
 
-/* Resident CTAs of the batch kernel on the current device (the default persistent grid). */
+/* Resident CTAs of the 128-thread batch kernel (classes 256 ... 2048) on the current device (its
+ * default persistent grid). */
 SP_API int sp_batch_max_grid(void);
 
-/* Launch a batch from its device descriptor table (grid <= 0: resident maximum). The first run on
- * a device builds a twiddle table and must not be inside a stream capture. */
+/* Launch a batch from its device descriptor table: the 4096-point class on a 256-thread
+ * persistent kernel (resident maximum), then the other classes on the 128-thread kernel (grid
+ * CTAs; grid <= 0: resident maximum) as its programmatic dependent. The first run on a device
+ * builds a twiddle table and must not be inside a stream capture. */
 SP_API int sp_batch_run(const void* desc_dev, void* ws, int grid, void* stream);
 
 #ifdef __cplusplus

@@ -4,9 +4,10 @@ channels).
 The schedule knob of the batch kernel is the work of one team task: segments per task for welch
 requests (each task then writes one partial row, so larger tasks mean less partial traffic and
 fewer counter atomics, smaller tasks a shorter tail), frames per task for streaming-STFT chunks.
-The FFT radix sequence is fixed per nperseg by the 128-thread CTA shape (teams of P = L/E
-threads, E = 32 points per thread from L = 512 up, 16 at L = 256), and the grid is the resident
-maximum (the queue balances it). A schedule changes only how work is cut, never which
+The FFT radix sequence is fixed per nperseg by the CTA shape (teams of P = L/E threads, E = 32
+points per thread at L = 1024 and 16 at the other classes; 128-thread CTAs up to L = 2048, one
+256-thread team per CTA at 4096), and the grids are the resident maxima (the queues balance
+them). A schedule changes only how work is cut, never which
 arithmetic is done; a request's result is bit-identical under every schedule only up to the
 grouping of its partial sums, so the schedule of a request depends on its own
 (kind, nperseg, dtype, channels) key, never on the other requests of a batch -- a request gives

@@ -1,5 +1,6 @@
-"""Batched spectral requests: many welch calls and streaming-STFT chunks in ONE persistent
-kernel launch over a device work queue (C-ABI sp_batch_*, include/b200signal.h).
+"""Batched spectral requests: many welch calls and streaming-STFT chunks in ONE batched launch
+(`sp_batch_run`: a persistent kernel for the 4096-point class, then one for the other classes as
+its programmatic dependent) over a device work queue (C-ABI sp_batch_*, include/b200signal.h).
 
 * `prepare_welch(x, **welch_kwargs)` validates one welch call exactly as `welch` does and, when
   it fits the batched kernel (real input, nperseg == nfft in {256, 512, 1024, 2048, 4096}, 50% overlap,
@@ -10,8 +11,8 @@ kernel launch over a device work queue (C-ABI sp_batch_*, include/b200signal.h).
   concatenation of all chunk outputs equals scipy.signal.stft of the concatenated stream with
   boundary=None, padded=False.
 * `BatchLauncher` owns the device workspace and descriptor slots (pinned host + device copy per
-  slot, one CUDA stream per slot) and launches a list of jobs as one kernel, replayed from a
-  captured CUDA graph after the first launch of a slot.
+  slot, one CUDA stream per slot) and launches a list of jobs as one batched launch, replayed
+  from a captured CUDA graph after the first launch of a slot.
 * `welch_batch(signals, **kw)` is the one-shot form: one launch for the eligible requests, the
   regular `welch` for the rest.
 
@@ -143,9 +144,10 @@ def _tables(window, nperseg: int) -> _Tables | None:
 
 
 def _batch_team(nperseg: int) -> int:
-    """Threads per FFT team of the batched kernel's class (32 points per thread at 1024 and 4096,
-    16 at 256 and 512): the low window-spectrum bins its constant-detrend correction can apply."""
-    return nperseg // (32 if nperseg in (1024, 4096) else 16)
+    """Threads per FFT team of the batched kernels' class (32 points per thread at 1024, 16 at
+    256, 512, 2048 and 4096): the low window-spectrum bins its constant-detrend correction can
+    apply."""
+    return nperseg // (32 if nperseg == 1024 else 16)
 
 
 def _rows_view(X: torch.Tensor) -> tuple[torch.Tensor, int]:
@@ -392,7 +394,7 @@ def _as_array(reqs):
 
 
 class BatchLauncher:
-    """Launch batches of jobs as one persistent kernel each.
+    """Launch batches of jobs as one batched launch (`sp_batch_run`) each.
 
     Each slot owns a CUDA stream, a zero-initialised workspace (queue, row counters, partial
     sums), and a descriptor buffer pair (pinned host, device). A launch picks the next slot

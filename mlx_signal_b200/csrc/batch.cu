@@ -1,5 +1,5 @@
 // C-ABI and kernel entry of the persistent batched launch (welch requests and streaming-STFT
-// chunks of uneven size and segment length in one launch over a device work queue).
+// chunks of uneven size and segment length in one batched launch over device work queues).
 #include <algorithm>
 #include <mutex>
 #include <numeric>
@@ -11,23 +11,58 @@
 
 namespace b2s {
 
-// Inter-pass twiddles of the 4096-point class, which do not fit the shared-memory union; built
-// once per device by k_batch_init (FP64 sincospi, rounded once, as the shared tables).
-using BatchPlan12 = Plan<12, batch_log_e<12>()>;
-__device__ float2 g_batch_tw12[BatchPlan12::TW];
-// the 2048 class's inter-pass twiddles exceed the shared-memory twiddle slot as well
+// Inter-pass twiddles of the 2048-point class, which exceed the 128-thread kernel's shared
+// twiddle slot; built once per device by k_batch_init (FP64 sincospi, rounded once, as the
+// shared tables).
 using BatchPlan11 = Plan<11, batch_log_e<11>()>;
 __device__ float2 g_batch_tw11[BatchPlan11::TW];
 
 __global__ void k_batch_init() {
-  build_twiddles<BatchPlan12>(g_batch_tw12, int(blockIdx.x * blockDim.x + threadIdx.x),
-                              int(gridDim.x * blockDim.x));
   build_twiddles<BatchPlan11>(g_batch_tw11, int(blockIdx.x * blockDim.x + threadIdx.x),
                               int(gridDim.x * blockDim.x));
 }
 
 constexpr int kBatchMinBlocks = 3;
+constexpr int kBatchBigMinBlocks = 2;
 
+// Queue words (int): [0] next item and [1] CTAs finished of the 128-thread kernel, [2] and [3]
+// the same for the 256-thread kernel.
+__device__ __forceinline__ void batch_take(const BatchParams& bp, int* qnext, int first, int end,
+                                           int nreq, int* s_item, int* s_req) {
+  if (threadIdx.x == 0) {
+    const int it = first + atomicAdd(qnext, 1);
+    const int* item_begin = reinterpret_cast<const int*>(bp.desc + sizeof(BatchHeader));
+    int lo = 0;
+    if (it < end) {  // largest request index with item_begin <= it
+      int hi = nreq - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ldg_i(item_begin + mid) <= it) lo = mid;
+        else hi = mid - 1;
+      }
+    }
+    *s_item = it;
+    *s_req = lo;
+  }
+  __syncthreads();
+}
+
+// The last CTA out of a kernel returns its two queue words to zero for the next launch.
+__device__ __forceinline__ void batch_finish(int* q) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(q + 1, 1) == int(gridDim.x) - 1) {
+      q[0] = 0;
+      q[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
+// Classes 256 ... 2048 (items [first_small, total)). Launched as a programmatic dependent of
+// k_batch_big: its CTAs take SMs as the 4096-class CTAs drain. The two kernels share no data
+// (disjoint requests, partial slots, row counters and queue words); each CTA waits for the
+// 4096-class grid before it exits, so the launch completes after both.
 __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) k_batch(BatchParams bp) {
   extern __shared__ float4 smem[];
   __shared__ int s_item, s_req, s_nrows;
@@ -36,6 +71,7 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) k_batch(BatchP
   const int* item_begin = reinterpret_cast<const int*>(bp.desc + sizeof(BatchHeader));
   const int nreq = ldg_i(&hdr->nreq);
   const int total = ldg_i(&hdr->total_items);
+  const int first = ldg_i(&hdr->first_small);
   const BatchReqDev* reqs = reinterpret_cast<const BatchReqDev*>(bp.desc + batch_req_offset(nreq));
   BatchTables cur;
   cur.log_l = -1;
@@ -43,45 +79,55 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchMinBlocks) k_batch(BatchP
   cur.wdft = nullptr;
   cur.n_low = -1;
   for (;;) {
-    if (threadIdx.x == 0) {
-      const int it = atomicAdd(bp.queue, 1);
-      int lo = 0;
-      if (it < total) {  // largest request index with item_begin <= it
-        int hi = nreq - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (ldg_i(item_begin + mid) <= it) lo = mid;
-          else hi = mid - 1;
-        }
-      }
-      s_item = it;
-      s_req = lo;
-    }
-    __syncthreads();
+    batch_take(bp, bp.queue, first, total, nreq, &s_item, &s_req);
     const int it = s_item;
     if (it >= total) break;
     const int ri = s_req;
     const BatchReqDev* rq = reqs + ri;
     const int local = it - ldg_i(item_begin + ri);
     switch (ldg_i(&rq->log_l)) {
-      case 8: batch_item<8, batch_log_e<8>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
-      case 9: batch_item<9, batch_log_e<9>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
-      case 10: batch_item<10, batch_log_e<10>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
-      case 11: batch_item<11, batch_log_e<11>()>(rq, local, smem, cur, g_batch_tw11, s_rows, &s_nrows); break;
-      case 12: batch_item<12, batch_log_e<12>()>(rq, local, smem, cur, g_batch_tw12, s_rows, &s_nrows); break;
-      default: break;  // rejected by the encoder
+      case 8: batch_item<8, batch_log_e<8>(), kBatchThreads, BatchSmall>(rq, local, smem, cur, g_batch_tw11, s_rows, &s_nrows); break;
+      case 9: batch_item<9, batch_log_e<9>(), kBatchThreads, BatchSmall>(rq, local, smem, cur, g_batch_tw11, s_rows, &s_nrows); break;
+      case 10: batch_item<10, batch_log_e<10>(), kBatchThreads, BatchSmall>(rq, local, smem, cur, g_batch_tw11, s_rows, &s_nrows); break;
+      case 11: batch_item<11, batch_log_e<11>(), kBatchThreads, BatchSmall>(rq, local, smem, cur, g_batch_tw11, s_rows, &s_nrows); break;
+      default: break;  // the encoder places the 4096 class before first_small
     }
     __syncthreads();
   }
-  // The last CTA out returns the queue to its initial state for the next launch.
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(bp.queue + 1, 1) == int(gridDim.x) - 1) {
-      bp.queue[0] = 0;
-      bp.queue[1] = 0;
-      __threadfence();
-    }
+  pdl_wait();
+  batch_finish(bp.queue);
+}
+
+// The 4096-point class (items [0, first_small)): one 256-thread team per CTA, 16 points per thread,
+// every table in shared memory. Starts its dependent (k_batch) at once.
+__global__ void __launch_bounds__(kBatchBigThreads, kBatchBigMinBlocks) k_batch_big(BatchParams bp) {
+  extern __shared__ float4 smem[];
+  __shared__ int s_item, s_req, s_nrows;
+  __shared__ int s_rows[16];
+  pdl_trigger();
+  const BatchHeader* hdr = reinterpret_cast<const BatchHeader*>(bp.desc);
+  const int* item_begin = reinterpret_cast<const int*>(bp.desc + sizeof(BatchHeader));
+  const int nreq = ldg_i(&hdr->nreq);
+  const int end = ldg_i(&hdr->first_small);
+  const BatchReqDev* reqs = reinterpret_cast<const BatchReqDev*>(bp.desc + batch_req_offset(nreq));
+  BatchTables cur;
+  cur.log_l = -1;
+  cur.win = nullptr;
+  cur.wdft = nullptr;
+  cur.n_low = -1;
+  for (;;) {
+    batch_take(bp, bp.queue + 2, 0, end, nreq, &s_item, &s_req);
+    const int it = s_item;
+    if (it >= end) break;
+    const int ri = s_req;
+    const BatchReqDev* rq = reqs + ri;
+    const int local = it - ldg_i(item_begin + ri);
+    if (ldg_i(&rq->log_l) == 12)
+      batch_item<12, batch_log_e<12>(), kBatchBigThreads, BatchBig>(rq, local, smem, cur, nullptr,
+                                                                    s_rows, &s_nrows);
+    __syncthreads();
   }
+  batch_finish(bp.queue + 2);
 }
 
 namespace {
@@ -299,7 +345,7 @@ int sp_batch_encode(const sp_batch_request* reqs, int nreq, void* ws, size_t ws_
   hdr->magic = kBatchMagic;
   hdr->nreq = nreq;
   hdr->total_items = int(items);
-  hdr->pad = 0;
+  hdr->first_small = 0;
   int* ib = reinterpret_cast<int*>(blob + sizeof(BatchHeader));
   BatchReqDev* rd = reinterpret_cast<BatchReqDev*>(blob + batch_req_offset(nreq));
   unsigned char* wsb = static_cast<unsigned char*>(ws);
@@ -316,6 +362,7 @@ int sp_batch_encode(const sp_batch_request* reqs, int nreq, void* ws, size_t ws_
     const ReqPlan& p = plans[size_t(i)];
     ib[j] = item;
     item += p.items;
+    if (p.log_l == 12) hdr->first_small = item;  // the class sorts first (batch_order)
     BatchReqDev d = {};
     d.x = r.x;
     d.win = r.win;
@@ -386,22 +433,42 @@ int sp_batch_run(const void* desc_dev, void* ws, int grid, void* stream) {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(kBatchSmemBytes)),
                      "cudaFuncSetAttribute(k_batch)");
-      k_batch_init<<<33, 128, 0, s>>>();
+      B2S_CHECK_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(k_batch_big),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(kBatchBigSmemBytes)),
+                     "cudaFuncSetAttribute(k_batch_big)");
+      k_batch_init<<<17, 128, 0, s>>>();
       B2S_CHECK_CUDA(cudaGetLastError(), "batch table init");
       g_batch_ready[dev] = true;
     }
   }
   const int maxg = sp_batch_max_grid();
-  if (maxg <= 0) {
-    set_error("no resident CTA for the batch kernel");
+  int sms = 0;
+  const int nbig = resident_ctas(reinterpret_cast<const void*>(k_batch_big), kBatchBigThreads,
+                                 kBatchBigSmemBytes, &sms);
+  if (maxg <= 0 || nbig <= 0) {
+    set_error("no resident CTA for the batch kernels");
     return SP_ERR_UNSUPPORTED;
   }
   if (grid <= 0 || grid > maxg) grid = maxg;
   BatchParams bp;
   bp.desc = static_cast<const unsigned char*>(desc_dev);
   bp.queue = static_cast<int*>(ws);
-  k_batch<<<grid, kBatchThreads, kBatchSmemBytes, s>>>(bp);
-  B2S_CHECK_CUDA(cudaGetLastError(), "batch kernel launch");
+  // the 4096 class first (its CTAs start the dependent launch at once), then the other classes
+  // as a programmatic dependent that fills SMs as the first kernel's CTAs finish
+  k_batch_big<<<nbig * sms, kBatchBigThreads, kBatchBigSmemBytes, s>>>(bp);
+  B2S_CHECK_CUDA(cudaGetLastError(), "batch kernel launch (4096 class)");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(grid));
+  cfg.blockDim = dim3(unsigned(kBatchThreads));
+  cfg.dynamicSmemBytes = kBatchSmemBytes;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  B2S_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_batch, bp), "batch kernel launch");
   return SP_OK;
 }
 

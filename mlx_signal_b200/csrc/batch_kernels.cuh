@@ -1,14 +1,18 @@
-// Persistent batched kernel: many independent spectral requests of uneven size and segment length
-// in ONE launch, pulled from a device work queue.
+// Persistent batched kernels: many independent spectral requests of uneven size and segment
+// length in ONE batched launch (two persistent grids over one descriptor table), pulled from
+// device work queues.
 //
 // Work model. The host encodes a descriptor table: a header, the first work item of every request
 // (item_begin, an exclusive prefix over requests) and one BatchReqDev per request. A request's
 // work is split into team tasks (a contiguous range of segments of one row, or of frame pairs of
 // one stream chunk); TEAMS consecutive tasks of one request form a CTA work item. Each CTA takes
 // the next item with an atomic on the queue head, finds its request by binary search over
-// item_begin, switches to the request's FFT class (L = 256, 512, 1024 or 4096) and runs the same
-// register/shared-memory team FFT as the single-request kernels. Tables (window, low-bin window
-// spectrum, twiddles) are reloaded only when the class or the window changes between items.
+// item_begin, switches to the request's FFT class (L = 256, 512, 1024, 2048 or 4096) and runs the
+// same register/shared-memory team FFT as the single-request kernels. Tables (window, low-bin
+// window spectrum, twiddles) are reloaded only when the class or the window changes between items.
+// Two persistent kernels share the descriptor table: the 4096 class (sorted first, items
+// [0, first_small)) runs one 256-thread team per CTA, 16 points per thread, the shape of the
+// single-request 4096 kernel; the other classes run on 128-thread CTAs (teams of 32 or 128).
 //
 // Welch requests (hop = L/2, the reference's default noverlap) use the half-overlap pair loop of
 // the single-request welch kernel, with the spectral form of the constant detrend (a zero
@@ -58,7 +62,7 @@ struct alignas(16) BatchHeader {
   int magic;
   int nreq;
   int total_items;
-  int pad;
+  int first_small;  // items [0, first_small) are the 4096-point class (256-thread kernel)
 };
 constexpr int kBatchMagic = 0x42415443;  // "BATC"
 
@@ -75,18 +79,26 @@ struct BatchParams {
   int* queue;  // [0] next item, [1] CTAs finished
 };
 
-constexpr int kBatchThreads = 128;
-// Shared-memory union over the classes (float4 units): scratch 8 | window 4096 floats | low bins
-// 2 x 128 complex | twiddles 1024 complex (classes <= 1024; 4096 reads a global table) |
-// exchange buffers 4224 complex (TEAMS x BUF of every class).
-constexpr int kBatchScratchF4 = 8;
-constexpr int kBatchWinFloats = 4096;
-constexpr int kBatchLowBins = 128;
-constexpr int kBatchTwSmem = 1024;
-constexpr int kBatchBufC = 4224;
-constexpr size_t kBatchSmemBytes = size_t(kBatchScratchF4) * 16 + size_t(kBatchWinFloats) * 4 +
-                                   size_t(2 * kBatchLowBins) * 8 + size_t(kBatchTwSmem) * 8 +
-                                   size_t(kBatchBufC) * 8;
+constexpr int kBatchThreads = 128;     // classes 256 ... 2048: teams of 32 or 128 threads
+constexpr int kBatchBigThreads = 256;  // class 4096: one 256-thread team, 16 points per thread
+
+// Shared-memory layout of a batched kernel (float4 units for the scratch, element counts for the
+// rest): scratch | window | low-bin window spectrum (2 x LOWB complex) | twiddles (TWC complex:
+// every class whose table fits; larger ones read a global table) | exchange buffers (BUFC complex,
+// TEAMS x BUF of every class the kernel runs).
+template <int SCR_F4, int WINF, int LOWB, int TWC, int BUFC>
+struct BatchLayout {
+  static constexpr int kScratchF4 = SCR_F4, kWinFloats = WINF, kLowBins = LOWB, kTwSmem = TWC,
+                       kBufC = BUFC;
+  static constexpr size_t kBytes = size_t(SCR_F4) * 16 + size_t(WINF) * 4 + size_t(2 * LOWB) * 8 +
+                                   size_t(TWC) * 8 + size_t(BUFC) * 8;
+};
+// 128-thread kernel: twiddles of the classes <= 1024 in shared memory (2048 reads a global table)
+using BatchSmall = BatchLayout<8, 4096, 128, 1024, 4224>;
+// 256-thread kernel (Plan<12, 4>: three radix-16 passes): every table in shared memory
+using BatchBig = BatchLayout<8, 4096, 256, 4352, 4352>;
+constexpr size_t kBatchSmemBytes = BatchSmall::kBytes;
+constexpr size_t kBatchBigSmemBytes = BatchBig::kBytes;
 
 __device__ __forceinline__ int ldg_i(const int* p) { return __ldg(p); }
 
@@ -120,7 +132,9 @@ struct BatchTables {
   int n_low;
 };
 
-template <int LOG_L, int LOG_E>
+// One CTA work item of request rq (item `local` of the request) with class (LOG_L, LOG_E) on an
+// NT-thread CTA whose shared memory has layout LAY.
+template <int LOG_L, int LOG_E, int NT, class LAY>
 __device__ __forceinline__ void batch_item(const BatchReqDev* __restrict__ rq, int local,
                                            float4* smem, BatchTables& cur,
                                            const float2* __restrict__ tw_global, int* s_rows,
@@ -128,16 +142,16 @@ __device__ __forceinline__ void batch_item(const BatchReqDev* __restrict__ rq, i
   using CFG = MeanCfg<LOG_L, LOG_E>;
   using PL = typename CFG::PL;
   constexpr int L = PL::L, E = PL::E, P = PL::P;
-  static_assert(CFG::THREADS == kBatchThreads, "batch classes use 128-thread CTAs");
-  static_assert(CFG::TEAMS * CFG::SCRATCH <= kBatchScratchF4, "scratch");
-  static_assert(CFG::TEAMS * PL::BUF <= kBatchBufC, "exchange buffers");
-  static_assert(P <= kBatchLowBins && L <= kBatchWinFloats, "tables");
-  constexpr bool kTwInSmem = PL::TW <= kBatchTwSmem;
-  float* win = reinterpret_cast<float*>(smem + kBatchScratchF4);
-  float2* wlo = reinterpret_cast<float2*>(win + kBatchWinFloats);
-  float2* whi = wlo + kBatchLowBins;
-  float2* tws = whi + kBatchLowBins;
-  float2* bufs = tws + kBatchTwSmem;
+  static_assert(CFG::THREADS == NT, "class and kernel CTA size differ");
+  static_assert(CFG::TEAMS * CFG::SCRATCH <= LAY::kScratchF4, "scratch");
+  static_assert(CFG::TEAMS * PL::BUF <= LAY::kBufC, "exchange buffers");
+  static_assert(P <= LAY::kLowBins && L <= LAY::kWinFloats, "tables");
+  constexpr bool kTwInSmem = PL::TW <= LAY::kTwSmem;
+  float* win = reinterpret_cast<float*>(smem + LAY::kScratchF4);
+  float2* wlo = reinterpret_cast<float2*>(win + LAY::kWinFloats);
+  float2* whi = wlo + LAY::kLowBins;
+  float2* tws = whi + LAY::kLowBins;
+  float2* bufs = tws + LAY::kTwSmem;
   const int tid = threadIdx.x;
 
   const int kind = ldg_i(&rq->kind);
@@ -146,19 +160,19 @@ __device__ __forceinline__ void batch_item(const BatchReqDev* __restrict__ rq, i
   const int nl = kind == kBatchWelch ? ldg_i(&rq->n_low) : 0;
   bool reload = false;
   if (cur.log_l != LOG_L) {
-    if constexpr (kTwInSmem) build_twiddles<PL>(tws, tid, kBatchThreads);
+    if constexpr (kTwInSmem) build_twiddles<PL>(tws, tid, NT);
     cur.log_l = LOG_L;
     cur.win = nullptr;
     cur.n_low = -1;
     reload = true;
   }
   if (cur.win != w) {
-    for (int i = tid; i < L; i += kBatchThreads) win[i] = __ldg(w + i);
+    for (int i = tid; i < L; i += NT) win[i] = __ldg(w + i);
     cur.win = w;
     reload = true;
   }
   if (cur.wdft != wd || cur.n_low != nl) {
-    load_window_lowbins<P>(wlo, whi, wd, nl, tid, kBatchThreads);
+    load_window_lowbins<P>(wlo, whi, wd, nl, tid, NT);
     cur.wdft = wd;
     cur.n_low = nl;
     reload = true;
@@ -227,7 +241,7 @@ __device__ __forceinline__ void batch_item(const BatchReqDev* __restrict__ rq, i
         const int row = s_rows[i];
         const float* q = rq->part + int64_t(row) * chunks * SLOT;
         float* o = rq->out + int64_t(row) * nbins;
-        for (int k = tid; k < nbins; k += kBatchThreads) {
+        for (int k = tid; k < nbins; k += NT) {
           const int kc = k <= L / 2 ? k : L - k;
           const float* qk = q + kc;
           // eight independent FP64 sums keep eight L2 loads in flight per thread (this reduce

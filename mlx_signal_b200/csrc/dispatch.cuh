@@ -23,10 +23,11 @@ constexpr int team_log_e() {
   return LOG_L <= 5 ? LOG_L : (LOG_L == 6 ? 3 : (LOG_L == 10 ? 5 : 4));
 }
 
-// Points per thread of the batched kernel's classes (128-thread CTAs: 32 points at L = 4096).
+// Points per thread of the batched kernels' classes: the single-request team shapes (the 4096
+// class runs in its own 256-thread kernel, 16 points per thread).
 template <int LOG_L>
 constexpr int batch_log_e() {
-  return LOG_L == 12 ? 5 : team_log_e<LOG_L>();
+  return team_log_e<LOG_L>();
 }
 
 constexpr int kMaxLogL = 12;
@@ -38,7 +39,7 @@ constexpr int kMaxLogLReal = 13;
 inline int team_log_e_rt(int log_l) {
   return log_l <= 5 ? log_l : (log_l == 6 ? 3 : (log_l == 10 ? 5 : 4));
 }
-inline int batch_log_e_rt(int log_l) { return log_l == 12 ? 5 : team_log_e_rt(log_l); }
+inline int batch_log_e_rt(int log_l) { return team_log_e_rt(log_l); }
 
 template <class P>
 using LaunchFnT = void (*)(dim3, int, size_t, cudaStream_t, const P&);

@@ -295,7 +295,6 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
     // other eleven powers by complex products in registers (each within ~2 ulp), a quarter of
     // the twiddle reads.
     constexpr bool kAnchors = L >= 2048 && Rn == 16;
-    constexpr bool kAnchors32 = L >= 2048 && Rn == 32;
     static_for<0, Bn>([&](auto bc) {
       constexpr int b = decltype(bc)::value;
       const int j = t + P * b;
@@ -304,18 +303,7 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
       // offset from pad(j)
       constexpr int QS = L / Rn;
       const float2* pj = buf + PL::pad(j);
-      float2 w1, w2, w3, w4, w5, w6, w7, w8, w16;
-      if constexpr (kAnchors32) {
-        w1 = twp[Sn + jm];
-        w2 = twp[2 * Sn + jm];
-        w4 = twp[4 * Sn + jm];
-        w8 = twp[8 * Sn + jm];
-        w16 = twp[16 * Sn + jm];
-        w3 = cmul(w1, w2);
-        w5 = cmul(w4, w1);
-        w6 = cmul(w4, w2);
-        w7 = cmul(w4, w3);
-      }
+      float2 w1, w2, w3, w4, w5, w6, w7, w8;
       if constexpr (kAnchors) {
         w1 = twp[Sn + jm];
         w2 = twp[2 * Sn + jm];
@@ -335,15 +323,7 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
           val = buf[PL::pad(j + q * QS)];
         }
         if constexpr (q > 0) {
-          if constexpr (kAnchors32) {
-            constexpr int lo = q & 7;
-            const float2 wl = lo == 1 ? w1 : lo == 2 ? w2 : lo == 3 ? w3 : lo == 4 ? w4
-                            : lo == 5 ? w5 : lo == 6 ? w6 : w7;
-            constexpr int m16 = q & 15;
-            const float2 w15 = m16 == 8 ? w8 : (m16 > 8 ? cmul(w8, wl) : wl);  // w^(q mod 16)
-            const float2 wq = q == 16 ? w16 : (q > 16 ? cmul(w16, w15) : w15);
-            val = cmul(val, wq);
-          } else if constexpr (kAnchors) {
+          if constexpr (kAnchors) {
             constexpr int lo = q & 7;
             const float2 wl = lo == 1 ? w1 : lo == 2 ? w2 : lo == 3 ? w3 : lo == 4 ? w4
                             : lo == 5 ? w5 : lo == 6 ? w6 : w7;

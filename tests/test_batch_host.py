@@ -175,6 +175,8 @@ def test_descriptor_layout_and_order(rng):
     assert np.all(np.diff(recs["log_l"]) <= 0)
     items = np.diff(ib)
     assert ib[0] == 0 and hdr[2] == ib[-1]
+    # the 4096 class (the 256-thread kernel's work) holds items [0, first_small)
+    assert hdr[3] == ib[int(np.sum(recs["log_l"] == 12))]
     for rec, it in zip(recs, items):
         assert it == -(-int(rec["tasks"]) // TEAMS[int(rec["log_l"])])
         assert rec["tasks"] == rec["rows"] * rec["chunks"]
