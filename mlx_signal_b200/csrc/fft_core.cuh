@@ -303,7 +303,7 @@ __device__ __forceinline__ void team_passes(float2 (&v)[PL::E], float2* buf, con
       // offset from pad(j)
       constexpr int QS = L / Rn;
       const float2* pj = buf + PL::pad(j);
-      float2 w1, w2, w3, w4, w5, w6, w7, w8;
+      [[maybe_unused]] float2 w1, w2, w3, w4, w5, w6, w7, w8;  // set only with kAnchors
       if constexpr (kAnchors) {
         w1 = twp[Sn + jm];
         w2 = twp[2 * Sn + jm];

@@ -317,7 +317,7 @@ __device__ __forceinline__ void welch_half_range(const HalfCtx<PL>& c, const flo
       B[gi] = __ldg(base + H + n);
       C[gi] = TWO ? __ldg(base + 2 * H + n) : 0.f;
     });
-    float ma = 0.f, mb = 0.f;
+    [[maybe_unused]] float ma = 0.f, mb = 0.f;  // segment means (constant detrend only)
     if constexpr (DET == kDetrendConstant || DET == kDetrendConstantSpectral) {
       // block totals: A's comes from the previous pair (its C), so only B and C are reduced
       float sa = sum_c;
