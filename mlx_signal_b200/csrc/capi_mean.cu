@@ -200,8 +200,8 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
   } else if (cross) {
     pl->k = canon = mean_lookup_cross(log_l, detrend);
   } else if (half) {
-    pl->k = mean_lookup_welch_half(log_l, hdet);
-    canon = mean_lookup_welch_half(log_l, detrend);
+    pl->k = mean_lookup_welch_half(log_l, hdet, false);
+    canon = mean_lookup_welch_half(log_l, detrend, false);
   } else {
     pl->k = canon = mean_lookup_welch(log_l, detrend);
   }
@@ -225,6 +225,9 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
           : cross ? cdiv(total, int64_t(waves) * cap)
                   : 2 * cdiv(total, 2 * int64_t(waves) * cap);
   if (pl->G < 1) pl->G = 1;
+  // long team ranges sum through shared-memory block totals (same shape, threads and smem)
+  if (half && !cross && !cplx && !blue && pl->G > kDirectSegs)
+    pl->k = mean_lookup_welch_half(log_l, hdet, true);
   pl->nteams = cdiv(total, pl->G);
   pl->blocks = cdiv(pl->nteams, pl->k.teams);
   int64_t cm = cdiv(pl->nseg, pl->G) + 1;

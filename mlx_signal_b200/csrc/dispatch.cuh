@@ -66,7 +66,8 @@ constexpr int kBlueIstftMaxN = 2048;
 // (log_l in [0, kMaxLogLReal] for the real-input families below)
 MeanInfo mean_lookup_welch(int log_l, int det);
 MeanInfo mean_lookup_cross(int log_l, int det);
-MeanInfo mean_lookup_welch_half(int log_l, int det);  // det 0/1/2(spectral), log_l >= 1
+// det 0/1/2(spectral), log_l >= 1; blocked: the instantiation with shared-memory block totals
+MeanInfo mean_lookup_welch_half(int log_l, int det, bool blocked);
 MeanInfo mean_lookup_cross_half(int log_l, int det, bool csd);  // det 0/1/2(spectral)
 FrameInfo frame_lookup_stft(int log_l, int det);
 FrameInfo frame_lookup_power(int log_l, int det);

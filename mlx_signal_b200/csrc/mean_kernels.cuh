@@ -99,6 +99,13 @@ __host__ __device__ constexpr int welch_slot_floats(int L) { return L / 2 + 1; }
 // kFoldPairs + pairs / kFoldPairs instead of with the number of pairs; the cross-team sum of the
 // partial slots is FP64 (k_reduce_mean).
 constexpr int kFoldPairs = 8;
+// From nfft 2048 up the 50%-overlap welch kernel keeps plain FP32 register sums while a team's
+// range holds at most kDirectPairs pairs (relative rounding error <= kDirectPairs * 2^-24 ~
+// 3.8e-6) and adds the shared-memory block totals only beyond that (the BLOCKED instantiation,
+// chosen by the host from the segments per team): the totals cost 3-5 % of the kernel's time at
+// nperseg 4096 and 8192 on 64 x 2^20, whose teams sum ~110 segments.
+constexpr int kDirectPairs = 64;
+constexpr int kDirectSegs = 2 * kDirectPairs;  // host switch: block totals when G > kDirectSegs
 
 template <int E, int P>
 __device__ __forceinline__ void fold_block(float (&acc)[E], float* tot, int t) {
@@ -407,7 +414,7 @@ __device__ __forceinline__ void load_window_lowbins(float2* lo, float2* hi, cons
   }
 }
 
-template <int LOG_L, int LOG_E, int DET>
+template <int LOG_L, int LOG_E, int DET, bool BLOCKED>
 __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L, LOG_E>::MIN_CTAS)
     k_welch_half(MeanParams pr) {
   using CFG = MeanCfg<LOG_L, LOG_E>;
@@ -449,7 +456,8 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
   const int64_t tau = int64_t(blockIdx.x) * CFG::TEAMS + team;
   int64_t g = tau * pr.G;
   const int64_t gend = min(g + pr.G, pr.total);
-  float* tot = reinterpret_cast<float*>(sbuf + CFG::TEAMS * PL::BUF) + team * L;
+  // block totals (BLOCKED: ranges longer than kDirectPairs pairs)
+  float* tot = BLOCKED ? reinterpret_cast<float*>(sbuf + CFG::TEAMS * PL::BUF) + team * L : nullptr;
   float acc[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) acc[e] = 0.f;
@@ -458,10 +466,12 @@ __global__ void __launch_bounds__(MeanCfg<LOG_L, LOG_E>::THREADS, MeanCfg<LOG_L,
     const int s0 = int(g - r * pr.nseg);
     const int64_t lim = int64_t(s0) + (gend - g);
     const int s1 = int(lim < pr.nseg ? lim : int64_t(pr.nseg));
-    zero_total<E, P>(tot, c.t);
+    if constexpr (BLOCKED) zero_total<E, P>(tot, c.t);
     welch_half_range<PL, DET, WT>(c, pr.x + r * pr.ld_x, s0, s1, acc, tot);
+    if constexpr (BLOCKED) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) acc[e] += tot[e * P + c.t];
+      for (int e = 0; e < E; ++e) acc[e] += tot[e * P + c.t];
+    }
     const int64_t slot = tau - first_team(r, pr.nseg, pr.G);
     flush_mirror<PL>(acc, pr.partial + (r * pr.cmax + slot) * int64_t(welch_slot_floats(L)),
                      c.buf, c.t, c.mask);

@@ -485,20 +485,23 @@ def _welch_f64_chunked(x, nperseg, chunk_segments=1 << 15):
     return f, total / nseg
 
 
-def test_welch_long_channel_segment_sums():
-    """One 2^26-sample channel at nperseg 256 (524287 segments in a single row, ~150 per team):
-    the per-team segment sums are blocked (register blocks folded into a shared-memory total),
-    and the result stays within 1e-5 relative of float64 scipy on bins above 1e-6 of the peak,
-    for a tone-plus-noise input with a large dynamic range."""
+@pytest.mark.parametrize("nperseg", [256, 2048])
+def test_welch_long_channel_segment_sums(nperseg):
+    """One 2^26-sample channel in a single row, summed with register blocks folded into a
+    shared-memory total per team: at nperseg 256 (524287 segments, ~37 per team over four CTA
+    waves) and at nperseg 2048 (65535 segments over 444 single-team CTAs, ~148 per team: past
+    the 128-segment limit under which the nfft >= 2048 kernels keep plain register sums). Both
+    stay within 1e-5 relative of float64 scipy on bins above 1e-6 of the peak, for a
+    tone-plus-noise input with a large dynamic range."""
     n = 1 << 26
     g = torch.Generator(device="cuda")
     g.manual_seed(26)
     x = torch.randn(n, generator=g, device="cuda")
     t = torch.arange(n, device="cuda", dtype=torch.float64)
     x += (3.0 * torch.sin(2 * np.pi * 0.123 * t)).float()
-    _, p = msig.welch(x, nperseg=256)
+    _, p = msig.welch(x, nperseg=nperseg)
     xh = x.cpu().numpy()
-    _, pref = _welch_f64_chunked(xh, 256)
+    _, pref = _welch_f64_chunked(xh, nperseg)
     assert rel_err_bins(p.cpu().numpy(), pref) <= 1e-5
 
 
