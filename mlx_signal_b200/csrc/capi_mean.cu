@@ -225,9 +225,15 @@ int make_plan(int mode, int64_t rows, int64_t n, int nperseg, int nfft, int hop,
           : cross ? cdiv(total, int64_t(waves) * cap)
                   : 2 * cdiv(total, 2 * int64_t(waves) * cap);
   if (pl->G < 1) pl->G = 1;
-  // long team ranges sum through shared-memory block totals (same shape, threads and smem)
-  if (half && !cross && !cplx && !blue && pl->G > kDirectSegs)
+  // long team ranges sum through shared-memory block totals (same shape, threads and smem; the
+  // residency query also opts the kernel in to its dynamic shared memory)
+  if (half && !cross && !cplx && !blue && pl->G > kDirectSegs) {
     pl->k = mean_lookup_welch_half(log_l, hdet, true);
+    if (resident_ctas(pl->k.fn, pl->k.threads, pl->k.smem, &sms) <= 0) {
+      set_error("no resident CTA for spectral-mean kernel (nfft=%d, smem=%zu)", nfft, pl->k.smem);
+      return SP_ERR_UNSUPPORTED;
+    }
+  }
   pl->nteams = cdiv(total, pl->G);
   pl->blocks = cdiv(pl->nteams, pl->k.teams);
   int64_t cm = cdiv(pl->nseg, pl->G) + 1;

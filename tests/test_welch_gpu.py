@@ -487,12 +487,11 @@ def _welch_f64_chunked(x, nperseg, chunk_segments=1 << 15):
 
 @pytest.mark.parametrize("nperseg", [256, 2048])
 def test_welch_long_channel_segment_sums(nperseg):
-    """One 2^26-sample channel in a single row, summed with register blocks folded into a
-    shared-memory total per team: at nperseg 256 (524287 segments, ~37 per team over four CTA
-    waves) and at nperseg 2048 (65535 segments over 444 single-team CTAs, ~148 per team: past
-    the 128-segment limit under which the nfft >= 2048 kernels keep plain register sums). Both
-    stay within 1e-5 relative of float64 scipy on bins above 1e-6 of the peak, for a
-    tone-plus-noise input with a large dynamic range."""
+    """One 2^26-sample channel in a single row: at nperseg 256 (524287 segments, ~37 per team
+    over four CTA waves, register blocks folded into a shared-memory total) and at nperseg 2048
+    (65535 segments over 592 single-team CTAs, ~112 per team: plain FP32 register sums, within
+    the 128-segment limit of that form). Both stay within 1e-5 relative of float64 scipy on bins
+    above 1e-6 of the peak, for a tone-plus-noise input with a large dynamic range."""
     n = 1 << 26
     g = torch.Generator(device="cuda")
     g.manual_seed(26)
@@ -503,6 +502,23 @@ def test_welch_long_channel_segment_sums(nperseg):
     xh = x.cpu().numpy()
     _, pref = _welch_f64_chunked(xh, nperseg)
     assert rel_err_bins(p.cpu().numpy(), pref) <= 1e-5
+
+
+def test_welch_block_totals_at_large_nperseg():
+    """64 x 2^21 at nperseg 4096: 65472 segments over 296 single-team CTAs put ~222 segments in
+    each team's range, past the 128-segment limit of plain register sums, so the nfft >= 2048
+    kernel that folds register blocks into a shared-memory total runs; rows from both ends of
+    the grid match float64 scipy within 1e-5 on bins above 1e-6 of the peak."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(21)
+    x = torch.randn((64, 1 << 21), generator=g, device="cuda")
+    t = torch.arange(1 << 21, device="cuda", dtype=torch.float64)
+    x[::7] += (2.0 * torch.sin(2 * np.pi * 0.0371 * t)).float()
+    _, p = msig.welch(x, nperseg=4096)
+    rows = [0, 7, 40, 63]
+    xh = x[rows].cpu().numpy().astype(np.float64)
+    _, pref = sps.welch(xh, nperseg=4096)
+    assert rel_err_bins(p[rows].cpu().numpy(), pref) <= 1e-5
 
 
 def _csd_f64_chunked(x, y, nperseg, chunk_segments=1 << 15):
