@@ -7,7 +7,8 @@ namespace b2s {
 namespace {
 // BLOCKED: the instantiation with shared-memory block totals (long team ranges). The plain
 // register sums are used from nfft 2048 up, whose kernels are bound by shared-memory traffic
-// (measured 3-5 % faster at 4096 and 8192); nfft <= 1024 keeps the block totals in every case.
+// (measured 3-5 % faster at 4096 and 8192); nfft <= 1024 keeps the block totals in every case
+// (at 1024, FP32-bound, plain sums measured ~0.8 % slower).
 template <bool BLOCKED>
 struct Fam {
   template <int LOG_L, int DET>
